@@ -1,0 +1,208 @@
+"""flashgemm-b200: the reference flashgemm hot path (FP32 SGEMM and FP32 / BF16 /
+INT8 GEMM chains) on B200 tensor cores, behind the reference's own C entry points.
+
+This module is the Python-side mirror of that C ABI (ctypes over the in-tree
+libflashgemm_b200.so). The functions named like the reference's take the
+reference's arguments in the reference's order:
+
+    flashgemm_set_thread_num(num)                               flashgemm.h:19
+    flashgemm_multi_f32f32f32(C, B, N, num_gemm, A1, M1, K1, ...)      :21
+    flashgemm_multi_bf16bf16f32(C, B, N, num_gemm, A1, M1, K1, ...)    :23
+    flashgemm_multi_int8uint8int32(C, B, N, num_gemm, A1, M1, K1, ...) :25
+    LibShalom_sgemm_mp(transa, transb, C, A, B, M, N, K)        FP32_ID23.c:35
+
+with numpy arrays (host memory) for the matrices. Like the reference they
+return nothing; pass check=True to raise FlashgemmError on a failed call. The
+device-pointer entry points (chain_dev, sgemm_dev) take torch CUDA tensors.
+There is no CPU fallback: without the library or a B200, calls fail loudly.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libflashgemm_b200.so")
+
+FG_OK, FG_ERR_INVALID, FG_ERR_UNSUPPORTED, FG_ERR_CUDA, FG_ERR_NO_DEVICE, FG_ERR_TIMEOUT, \
+    FG_ERR_NOMEM = range(7)
+FG_SEM_REF, FG_SEM_MATH = 0, 1
+FG_F32_FFMA, FG_F32_3XTF32 = 0, 1
+FG_DT_F32, FG_DT_BF16, FG_DT_INT8 = 0, 1, 2
+_DT = {"f32": FG_DT_F32, "bf16": FG_DT_BF16, "int8": FG_DT_INT8}
+
+_P = ctypes.c_void_p
+_L = ctypes.c_long
+_lib = None
+
+
+class FlashgemmError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"flashgemm-b200 status {status}: {msg}")
+        self.status = status
+
+
+def lib():
+    """Load libflashgemm_b200.so (built by flashgemm_b200/build.py)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with `python flashgemm_b200/build.py`")
+        L = ctypes.CDLL(LIB_PATH)
+        L.fg_last_error.restype = ctypes.c_char_p
+        L.fg_version.restype = ctypes.c_char_p
+        L.fg_kernel_launches.restype = ctypes.c_ulonglong
+        for name in ("flashgemm_multi_f32f32f32", "flashgemm_multi_bf16bf16f32",
+                     "flashgemm_multi_int8uint8int32"):
+            f = getattr(L, name)
+            f.restype = None
+            f.argtypes = [_P, _P, _L, ctypes.c_int]  # then (ptr, long, long) triples
+        L.LibShalom_sgemm_mp.restype = None
+        L.LibShalom_sgemm_mp.argtypes = [ctypes.c_int, ctypes.c_int, _P, _P, _P, _L, _L, _L]
+        L.Small_NGM_NN_SGEMM.argtypes = [_P, _P, _P, _L, _L, _L, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int]
+        L.Small_MGN_NN_SGEMM.argtypes = L.Small_NGM_NN_SGEMM.argtypes
+        L.fg_chain_dev.argtypes = [ctypes.c_int, _P, _P, _L, ctypes.c_int, _P, _P, _P, _P]
+        L.fg_sgemm_dev.argtypes = [_P, _P, _P, _L, _L, _L, ctypes.c_int, _P]
+        _lib = L
+    return _lib
+
+
+def last_status():
+    return lib().fg_last_status()
+
+
+def last_error():
+    return lib().fg_last_error().decode()
+
+
+def _check(check):
+    st = lib().fg_last_status()
+    if check and st != FG_OK:
+        raise FlashgemmError(st, last_error())
+    return st
+
+
+def version():
+    return lib().fg_version().decode()
+
+
+def kernel_launches():
+    return int(lib().fg_kernel_launches())
+
+
+def set_semantics(sem):
+    lib().fg_set_semantics({"ref": FG_SEM_REF, "math": FG_SEM_MATH}.get(sem, sem))
+
+
+def get_semantics():
+    return lib().fg_get_semantics()
+
+
+def set_f32_algo(algo):
+    lib().fg_set_f32_algo({"ffma": FG_F32_FFMA, "3xtf32": FG_F32_3XTF32}.get(algo, algo))
+
+
+def set_sgemm_algo(algo):
+    lib().fg_set_sgemm_algo({"ffma": FG_F32_FFMA, "3xtf32": FG_F32_3XTF32}.get(algo, algo))
+
+
+def sync():
+    st = lib().fg_sync()
+    if st != FG_OK:
+        raise FlashgemmError(st, last_error())
+
+
+# ------------------------------------------------------------ reference entry points
+
+def _host_ptr(a, dtype):
+    if not isinstance(a, np.ndarray) or not a.flags["C_CONTIGUOUS"]:
+        raise TypeError("expected a C-contiguous numpy array")
+    if a.dtype != dtype:
+        raise TypeError(f"expected {np.dtype(dtype)}, got {a.dtype}")
+    return a.ctypes.data_as(_P)
+
+
+def _triples(args, adtype):
+    if len(args) % 3:
+        raise TypeError("weights come as (A_i, M_i, K_i) triples")
+    out = []
+    for i in range(0, len(args), 3):
+        A, M, K = args[i:i + 3]
+        out += [_host_ptr(A, adtype), _L(int(M)), _L(int(K))]
+    return out
+
+
+def flashgemm_set_thread_num(num):
+    lib().flashgemm_set_thread_num(int(num))
+
+
+def flashgemm_thread_num():
+    return ctypes.c_int.in_dll(lib(), "flashgemm_thread_num").value
+
+
+def flashgemm_multi_f32f32f32(C, B, N, num_gemm, *triples, check=False):
+    lib().flashgemm_multi_f32f32f32(_host_ptr(C, np.float32), _host_ptr(B, np.float32), int(N),
+                                    int(num_gemm), *_triples(triples, np.float32))
+    return _check(check)
+
+
+def flashgemm_multi_bf16bf16f32(C, B, N, num_gemm, *triples, check=False):
+    lib().flashgemm_multi_bf16bf16f32(_host_ptr(C, np.float32), _host_ptr(B, np.uint16), int(N),
+                                      int(num_gemm), *_triples(triples, np.uint16))
+    return _check(check)
+
+
+def flashgemm_multi_int8uint8int32(C, B, N, num_gemm, *triples, check=False):
+    lib().flashgemm_multi_int8uint8int32(_host_ptr(C, np.int32), _host_ptr(B, np.uint8), int(N),
+                                         int(num_gemm), *_triples(triples, np.int8))
+    return _check(check)
+
+
+def LibShalom_sgemm_mp(transa, transb, C, A, B, M, N, K, check=False):
+    lib().LibShalom_sgemm_mp(int(transa), int(transb), _host_ptr(C, np.float32),
+                             _host_ptr(A, np.float32), _host_ptr(B, np.float32), int(M), int(N),
+                             int(K))
+    return _check(check)
+
+
+def LibShalom_set_thread_nums(num):
+    lib().LibShalom_set_thread_nums(int(num))
+
+
+def Small_NGM_NN_SGEMM(C, A, B, M, N, K, NUM, Tm, Tn, check=False):
+    lib().Small_NGM_NN_SGEMM(_host_ptr(C, np.float32), _host_ptr(A, np.float32),
+                             _host_ptr(B, np.float32), int(M), int(N), int(K), NUM, Tm, Tn)
+    return _check(check)
+
+
+def Small_MGN_NN_SGEMM(C, A, B, M, N, K, NUM, Tm, Tn, check=False):
+    lib().Small_MGN_NN_SGEMM(_host_ptr(C, np.float32), _host_ptr(A, np.float32),
+                             _host_ptr(B, np.float32), int(M), int(N), int(K), NUM, Tm, Tn)
+    return _check(check)
+
+
+# ------------------------------------------------------------ device entry points
+
+def chain_dev(dtype, C, B, N, As, Ms, Ks, stream=None):
+    """Chain on torch CUDA tensors (contiguous). dtype: 'f32' | 'bf16' | 'int8'.
+    stream: a torch.cuda.Stream (default: torch's current stream)."""
+    import torch
+    n = len(As)
+    aptr = (_P * n)(*[a.data_ptr() for a in As])
+    ms = (ctypes.c_long * n)(*[int(m) for m in Ms])
+    ks = (ctypes.c_long * n)(*[int(k) for k in Ks])
+    s = (stream or torch.cuda.current_stream()).cuda_stream
+    st = lib().fg_chain_dev(_DT[dtype], C.data_ptr(), B.data_ptr(), int(N), n, aptr, ms, ks, s)
+    if st != FG_OK:
+        raise FlashgemmError(st, last_error())
+
+
+def sgemm_dev(C, A, B, M, N, K, algo="ffma", stream=None):
+    import torch
+    a = {"ffma": FG_F32_FFMA, "3xtf32": FG_F32_3XTF32}[algo]
+    s = (stream or torch.cuda.current_stream()).cuda_stream
+    st = lib().fg_sgemm_dev(C.data_ptr(), A.data_ptr(), B.data_ptr(), int(M), int(N), int(K), a, s)
+    if st != FG_OK:
+        raise FlashgemmError(st, last_error())

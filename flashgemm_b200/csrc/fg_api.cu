@@ -1,0 +1,736 @@
+// C ABI of flashgemm-b200: the reference's entry points (flashgemm.h,
+// libshalom.h) and the extension API (flashgemm_b200.h), over the CUDA kernels.
+//
+// Host code only. One context per device holds a stream, a grow-only scratch
+// arena and a device status word; a call takes the context's mutex, so calls
+// from several host threads are safe and serialised per device (the
+// reference's calls share global state and are not reentrant).
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/flashgemm.h"
+#include "../../include/flashgemm_b200.h"
+#include "../../include/libshalom.h"
+#include "fg_kernels.h"
+
+#define FG_EXPORT extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+using namespace fg;
+
+// ---------------------------------------------------------------- status
+
+thread_local int t_status = FG_OK;
+thread_local char t_msg[512] = "";
+
+int fail(int st, const char *fmt, ...)
+{
+    t_status = st;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(t_msg, sizeof t_msg, fmt, ap);
+    va_end(ap);
+    return st;
+}
+
+int ok()
+{
+    t_status = FG_OK;
+    t_msg[0] = 0;
+    return FG_OK;
+}
+
+#define CUDA_TRY(expr)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (expr);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return fail(FG_ERR_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_),    \
+                        __FILE__, __LINE__);                                             \
+    } while (0)
+
+// ---------------------------------------------------------------- settings
+
+int env_choice(const char *name, const char *a, int va, const char *b, int vb, int dflt)
+{
+    const char *v = getenv(name);
+    if (!v) return dflt;
+    if (!strcmp(v, a)) return va;
+    if (!strcmp(v, b)) return vb;
+    return dflt;
+}
+
+std::atomic<int> g_sem{-1}, g_f32{-1}, g_sgemm{-1};
+std::atomic<unsigned long long> g_launches{0};
+
+int semantics()
+{
+    int s = g_sem.load();
+    if (s < 0) {
+        s = env_choice("FG_SEMANTICS", "ref", FG_SEM_REF, "math", FG_SEM_MATH, FG_SEM_REF);
+        g_sem.store(s);
+    }
+    return s;
+}
+int f32_algo()
+{
+    int s = g_f32.load();
+    if (s < 0) {
+        s = env_choice("FG_F32_ALGO", "ffma", FG_F32_FFMA, "3xtf32", FG_F32_3XTF32, FG_F32_3XTF32);
+        g_f32.store(s);
+    }
+    return s;
+}
+int sgemm_algo()
+{
+    int s = g_sgemm.load();
+    if (s < 0) {
+        s = env_choice("FG_SGEMM_ALGO", "ffma", FG_F32_FFMA, "3xtf32", FG_F32_3XTF32, FG_F32_FFMA);
+        g_sgemm.store(s);
+    }
+    return s;
+}
+
+inline long round_up(long x, long a) { return (x + a - 1) / a * a; }
+
+// ---------------------------------------------------------------- per-device context
+
+struct DevCtx {
+    int dev = -1;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    std::mutex mu;
+    char *arena = nullptr;
+    size_t arena_cap = 0;
+    size_t arena_off = 0;
+    int *status = nullptr;       // device word the kernels report into
+    int *status_host = nullptr;  // pinned copy
+};
+
+std::mutex g_ctx_mu;
+DevCtx *g_ctx[64];
+
+int get_ctx(DevCtx **out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(FG_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+    }
+    if (dev < 0 || dev >= 64) return fail(FG_ERR_NO_DEVICE, "device index %d out of range", dev);
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    if (!g_ctx[dev]) {
+        cudaDeviceProp prop;
+        CUDA_TRY(cudaGetDeviceProperties(&prop, dev));
+        if (prop.major != 10)
+            return fail(FG_ERR_NO_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a",
+                        dev, prop.major, prop.minor);
+        DevCtx *c = new DevCtx;
+        c->dev = dev;
+        c->sms = prop.multiProcessorCount;
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming));
+        CUDA_TRY(cudaMalloc(&c->status, sizeof(int)));
+        CUDA_TRY(cudaMemset(c->status, 0, sizeof(int)));
+        CUDA_TRY(cudaMallocHost(&c->status_host, sizeof(int)));
+        g_ctx[dev] = c;
+    }
+    *out = g_ctx[dev];
+    return FG_OK;
+}
+
+// Scratch: ensure capacity (growing only while the stream is idle), then carve.
+int arena_reserve(DevCtx *c, size_t bytes)
+{
+    c->arena_off = 0;
+    if (bytes <= c->arena_cap) return FG_OK;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (c->arena) cudaFree(c->arena);
+    c->arena = nullptr;
+    c->arena_cap = 0;
+    size_t cap = bytes + bytes / 4 + (64u << 20);
+    cudaError_t e = cudaMalloc(&c->arena, cap);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(FG_ERR_NOMEM, "device scratch of %zu bytes: %s", cap, cudaGetErrorString(e));
+    }
+    c->arena_cap = cap;
+    return FG_OK;
+}
+
+void *arena_take(DevCtx *c, size_t bytes)
+{
+    size_t off = (c->arena_off + 255) & ~(size_t)255;
+    c->arena_off = off + bytes;
+    return c->arena + off;
+}
+
+size_t carve_size(size_t bytes) { return (bytes + 255) & ~(size_t)255; }
+
+// ---------------------------------------------------------------- chain core
+
+struct Mat {
+    const void *p;
+    long ld;
+};
+
+int elt_of(int dtype) { return dtype == FG_DT_INT8 ? 1 : dtype == FG_DT_BF16 ? 2 : 4; }
+
+int check_shapes(int dtype, long N, int n, const long *M, const long *K)
+{
+    if (n < 1) return fail(FG_ERR_INVALID, "num_gemm must be >= 1 (got %d)", n);
+    if (N < 0) return fail(FG_ERR_INVALID, "N must be >= 0");
+    for (int i = 0; i < n; ++i) {
+        if (M[i] <= 0 || K[i] <= 0)
+            return fail(FG_ERR_INVALID, "gemm %d: M and K must be positive", i + 1);
+        if (i > 0 && K[i] != M[i - 1])
+            return fail(FG_ERR_INVALID, "gemm %d: K (%ld) must equal the previous M (%ld)", i + 1,
+                        K[i], M[i - 1]);
+        if (M[i] > (1l << 30) || K[i] > (1l << 30) || N > (1l << 30))
+            return fail(FG_ERR_INVALID, "gemm %d: dimension too large", i + 1);
+    }
+    (void)dtype;
+    return FG_OK;
+}
+
+// Bytes of scratch a chain needs beyond its inputs and output.
+size_t chain_scratch(int dtype, int algo, long N, int n, const long *M, const long *K)
+{
+    const long ldN = round_up(N, 16);
+    size_t s = 0;
+    long maxM = 0;
+    for (int i = 0; i < n - 1; ++i) maxM = M[i] > maxM ? M[i] : maxM;
+    if (dtype == FG_DT_INT8) {
+        for (int i = 0; i < n; ++i) s += carve_size((size_t)M[i] * round_up(K[i] + 4, 16));
+        s += 2 * carve_size((size_t)maxM * ldN);
+    } else if (dtype == FG_DT_BF16) {
+        for (int i = 0; i < n; ++i)
+            if (K[i] % 8) s += carve_size((size_t)M[i] * round_up(K[i], 8) * 2);
+        s += 2 * carve_size((size_t)maxM * ldN * 2);
+    } else if (algo == FG_F32_3XTF32) {
+        for (int i = 0; i < n; ++i) s += 2 * carve_size((size_t)M[i] * round_up(K[i], 4) * 4);
+        s += 2 * carve_size((size_t)K[0] * ldN * 4);                 // split input
+        s += 2 * 2 * carve_size((size_t)maxM * ldN * 4);             // ping-pong hi/lo
+    } else {
+        s += 2 * carve_size((size_t)maxM * ldN * 4);
+    }
+    return s;
+}
+
+int launch(cudaError_t e, const char *what)
+{
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (e != cudaSuccess) return fail(FG_ERR_CUDA, "%s launch: %s", what, cudaGetErrorString(e));
+    return FG_OK;
+}
+
+// Runs the chain on c->stream. Device operands: B (K[0] x N, ld b.ld),
+// A[i] (M[i] x K[i], ld a[i].ld, 16-byte-aligned rows where the tensor path
+// needs them), C (M[n-1] x N, ld ldc). Scratch must already be reserved.
+int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b, long N, int n,
+              const Mat *a, const long *M, const long *K)
+{
+    const long ldN = round_up(N, 16);
+    const bool ref = (sem == FG_SEM_REF);
+    long maxM = 0;
+    for (int i = 0; i < n - 1; ++i) maxM = M[i] > maxM ? M[i] : maxM;
+
+    if (dtype == FG_DT_F32 && algo == FG_F32_FFMA) {
+        float *buf[2] = {nullptr, nullptr};
+        if (n > 1) {
+            buf[0] = (float *)arena_take(c, (size_t)maxM * ldN * 4);
+            buf[1] = (float *)arena_take(c, (size_t)maxM * ldN * 4);
+        }
+        const float *x = (const float *)b.p;
+        long ldx = b.ld;
+        for (int i = 0; i < n; ++i) {
+            FfmaArgs f;
+            f.M = (int)M[i]; f.N = (int)N; f.K = (int)K[i];
+            f.A = (const float *)a[i].p; f.lda = a[i].ld;
+            f.B = x; f.ldb = ldx;
+            const bool last = (i == n - 1);
+            f.C = last ? (float *)C : buf[i & 1];
+            f.ldc = last ? ldc : ldN;
+            f.kblock = 0;  // the multigemm FP32 chain does not split K (kernel_f32.h:3)
+            int st = launch(launch_ffma_sgemm(f, c->sms, c->stream), "ffma stage");
+            if (st) return st;
+            x = f.C;
+            ldx = f.ldc;
+        }
+        return FG_OK;
+    }
+
+    StageArgs s;
+    memset(&s, 0, sizeof s);
+    s.status = c->status;
+    s.N = (int)N;
+
+    if (dtype == FG_DT_F32) {  // 3xTF32
+        std::vector<float *> wh(n), wl(n);
+        for (int i = 0; i < n; ++i) {
+            const long ldk = round_up(K[i], 4);
+            wh[i] = (float *)arena_take(c, (size_t)M[i] * ldk * 4);
+            wl[i] = (float *)arena_take(c, (size_t)M[i] * ldk * 4);
+            int st = launch(launch_split_tf32((const float *)a[i].p, a[i].ld, wh[i], wl[i], ldk,
+                                              M[i], K[i], c->stream),
+                            "tf32 split (weights)");
+            if (st) return st;
+        }
+        float *xh = (float *)arena_take(c, (size_t)K[0] * ldN * 4);
+        float *xl = (float *)arena_take(c, (size_t)K[0] * ldN * 4);
+        int st = launch(launch_split_tf32((const float *)b.p, b.ld, xh, xl, ldN, K[0], N, c->stream),
+                        "tf32 split (activations)");
+        if (st) return st;
+        float *ph[2] = {nullptr, nullptr}, *pl[2] = {nullptr, nullptr};
+        if (n > 1)
+            for (int j = 0; j < 2; ++j) {
+                ph[j] = (float *)arena_take(c, (size_t)maxM * ldN * 4);
+                pl[j] = (float *)arena_take(c, (size_t)maxM * ldN * 4);
+            }
+        for (int i = 0; i < n; ++i) {
+            const bool last = (i == n - 1);
+            s.op = OP_TF32X3;
+            s.M = (int)M[i]; s.K = (int)K[i];
+            s.w = wh[i]; s.w_lo = wl[i]; s.ld_w = round_up(K[i], 4);
+            s.x = xh; s.x_lo = xl; s.ld_x = ldN;
+            s.epi = last ? EPI_F32 : EPI_TF32SPLIT;
+            s.out = last ? C : (void *)ph[i & 1];
+            s.out_lo = last ? nullptr : (void *)pl[i & 1];
+            s.ld_out = last ? ldc : ldN;
+            s.m_written = (int)M[i];
+            s.tail_lo = s.tail_hi = 0;
+            st = launch(launch_tc_stage(s, c->sms, c->stream), "tf32x3 stage");
+            if (st) return st;
+            xh = ph[i & 1];
+            xl = pl[i & 1];
+        }
+        return FG_OK;
+    }
+
+    if (dtype == FG_DT_BF16) {
+        uint16_t *buf[2] = {nullptr, nullptr};
+        if (n > 1) {
+            buf[0] = (uint16_t *)arena_take(c, (size_t)maxM * ldN * 2);
+            buf[1] = (uint16_t *)arena_take(c, (size_t)maxM * ldN * 2);
+        }
+        const void *x = b.p;
+        long ldx = b.ld;
+        for (int i = 0; i < n; ++i) {
+            const void *w = a[i].p;
+            long ldw = a[i].ld;
+            if ((ldw % 8) || ((uintptr_t)w % 16)) {
+                const long ldk = round_up(K[i], 8);
+                void *wp = arena_take(c, (size_t)M[i] * ldk * 2);
+                CUDA_TRY(cudaMemsetAsync(wp, 0, (size_t)M[i] * ldk * 2, c->stream));
+                CUDA_TRY(cudaMemcpy2DAsync(wp, ldk * 2, w, ldw * 2, K[i] * 2, M[i],
+                                           cudaMemcpyDeviceToDevice, c->stream));
+                w = wp;
+                ldw = ldk;
+            }
+            const bool last = (i == n - 1);
+            s.op = OP_BF16;
+            s.M = (int)M[i]; s.K = (int)K[i];
+            s.w = w; s.ld_w = ldw;
+            s.x = x; s.ld_x = ldx;
+            s.epi = last ? EPI_F32 : EPI_BF16;
+            s.out = last ? C : (void *)buf[i & 1];
+            s.ld_out = last ? ldc : ldN;
+            s.permute = ref ? 1 : 0;
+            s.m_written = (int)M[i];
+            s.tail_lo = s.tail_hi = 0;
+            int st = launch(launch_tc_stage(s, c->sms, c->stream), "bf16 stage");
+            if (st) return st;
+            x = s.out;
+            ldx = s.ld_out;
+        }
+        return FG_OK;
+    }
+
+    // INT8
+    {
+        uint8_t *buf[2] = {nullptr, nullptr};
+        if (n > 1) {
+            buf[0] = (uint8_t *)arena_take(c, (size_t)maxM * ldN);
+            buf[1] = (uint8_t *)arena_take(c, (size_t)maxM * ldN);
+        }
+        const void *x = b.p;
+        long ldx = b.ld;
+        for (int i = 0; i < n; ++i) {
+            const long Mi = M[i], Ki = K[i];
+            // reference tail rows (multigemm/src/kernel_int8.h:771-1057): only with
+            // whole k-quads; other K leave the reference undefined and get no shift
+            long tail_lo = 0, tail_hi = 0;
+            if (ref && Ki % 4 == 0 && Ki >= 4) {
+                tail_lo = (Mi / 12) * 12;
+                tail_hi = (Mi / 4) * 4;
+            }
+            const long ldw = round_up(Ki + 4, 16);
+            uint8_t *wp = (uint8_t *)arena_take(c, (size_t)Mi * ldw);
+            int st = launch(launch_prep_int8_weights((const int8_t *)a[i].p, a[i].ld, wp, ldw, Mi,
+                                                     Ki, tail_lo, tail_hi, c->stream),
+                            "int8 weight prep");
+            if (st) return st;
+            const bool last = (i == n - 1);
+            s.op = OP_I8;
+            s.M = (int)Mi; s.K = (int)Ki;
+            s.w = wp; s.ld_w = ldw;
+            s.x = x; s.ld_x = ldx;
+            s.epi = last ? EPI_S32 : EPI_S8;
+            s.out = last ? C : (void *)buf[i & 1];
+            s.ld_out = last ? ldc : ldN;
+            s.permute = ref ? 1 : 0;
+            s.m_written = (last && ref) ? (int)((Mi / 4) * 4) : (int)Mi;
+            s.tail_lo = (int)tail_lo;
+            s.tail_hi = (int)tail_hi;
+            st = launch(launch_tc_stage(s, c->sms, c->stream), "int8 stage");
+            if (st) return st;
+            x = s.out;
+            ldx = s.ld_out;
+        }
+        return FG_OK;
+    }
+}
+
+// Read and clear the device status word (the stream must be idle).
+int collect_status(DevCtx *c)
+{
+    CUDA_TRY(cudaMemcpyAsync(c->status_host, c->status, sizeof(int), cudaMemcpyDeviceToHost,
+                             c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const int code = *c->status_host;
+    if (code) {
+        CUDA_TRY(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        return fail(FG_ERR_TIMEOUT, "a kernel's pipeline wait ran out (code 0x%x)", code);
+    }
+    return FG_OK;
+}
+
+// Host-pointer chain: stage operands into device scratch, run, copy C back.
+int host_chain(int dtype, void *C, const void *B, long N, int n, const void *const *A,
+               const long *M, const long *K)
+{
+    int st = check_shapes(dtype, N, n, M, K);
+    if (st) return st;
+    for (int i = 0; i < n; ++i)
+        if (K[i] % 2 != 0) {
+            // same message and behaviour as the reference (flashgemm.c:13-22, :64-68)
+            printf("K must be a multiple of 2\n");
+            printf("Dimension error for gemm %d\n", i + 1);
+            return fail(FG_ERR_INVALID, "gemm %d: K must be a multiple of 2", i + 1);
+        }
+    if (N == 0) return ok();
+    DevCtx *c;
+    if ((st = get_ctx(&c))) return st;
+    std::lock_guard<std::mutex> lk(c->mu);
+    const int elt = elt_of(dtype);
+    const int sem = semantics();
+    const int algo = f32_algo();
+    const long ldN = round_up(N, 16);
+    const int out_elt = 4;
+    size_t need = carve_size((size_t)K[0] * ldN * elt) + carve_size((size_t)M[n - 1] * ldN * out_elt);
+    std::vector<long> lda(n);
+    for (int i = 0; i < n; ++i) {
+        lda[i] = round_up(K[i], 16 / elt);
+        need += carve_size((size_t)M[i] * lda[i] * elt);
+    }
+    need += chain_scratch(dtype, algo, N, n, M, K) + 4096;
+    if ((st = arena_reserve(c, need))) return st;
+
+    void *bd = arena_take(c, (size_t)K[0] * ldN * elt);
+    CUDA_TRY(cudaMemcpy2DAsync(bd, ldN * elt, B, N * elt, N * elt, K[0], cudaMemcpyHostToDevice,
+                               c->stream));
+    std::vector<Mat> ad(n);
+    for (int i = 0; i < n; ++i) {
+        void *p = arena_take(c, (size_t)M[i] * lda[i] * elt);
+        CUDA_TRY(cudaMemcpy2DAsync(p, lda[i] * elt, A[i], K[i] * elt, K[i] * elt, M[i],
+                                   cudaMemcpyHostToDevice, c->stream));
+        ad[i] = Mat{p, lda[i]};
+    }
+    void *cd = arena_take(c, (size_t)M[n - 1] * ldN * out_elt);
+    if ((st = run_chain(c, dtype, sem, algo, cd, ldN, Mat{bd, ldN}, N, n, ad.data(), M, K)))
+        return st;
+    // INT8 reference semantics leave rows >= 4 * floor(M / 4) of C untouched
+    // (multigemm/src/kernel_int8.h:943-945)
+    long rows = M[n - 1];
+    if (dtype == FG_DT_INT8 && sem == FG_SEM_REF) rows = (rows / 4) * 4;
+    if (rows > 0)
+        CUDA_TRY(cudaMemcpy2DAsync(C, N * out_elt, cd, ldN * out_elt, N * out_elt, rows,
+                                   cudaMemcpyDeviceToHost, c->stream));
+    if ((st = collect_status(c))) return st;
+    return ok();
+}
+
+int chain_va(int dtype, void *C, const void *B, long N, int num_gemm, va_list ap)
+{
+    if (num_gemm < 1 || num_gemm > 4096)
+        return fail(FG_ERR_INVALID, "num_gemm must be in [1, 4096] (got %d)", num_gemm);
+    std::vector<const void *> A(num_gemm);
+    std::vector<long> M(num_gemm), K(num_gemm);
+    for (int i = 0; i < num_gemm; ++i) {  // flashgemm.c:54-61: (T *A_i, long M_i, long K_i)
+        A[i] = va_arg(ap, const void *);
+        M[i] = va_arg(ap, long);
+        K[i] = va_arg(ap, long);
+    }
+    return host_chain(dtype, C, B, N, num_gemm, A.data(), M.data(), K.data());
+}
+
+// ---------------------------------------------------------------- SGEMM
+
+int run_sgemm(DevCtx *c, int algo, float *C, long ldc, const float *A, long lda, const float *B,
+              long ldb, long M, long N, long K, int kblock)
+{
+    if (algo == FG_F32_FFMA) {
+        FfmaArgs f;
+        f.M = (int)M; f.N = (int)N; f.K = (int)K;
+        f.A = A; f.lda = lda; f.B = B; f.ldb = ldb; f.C = C; f.ldc = ldc;
+        f.kblock = kblock;
+        return launch(launch_ffma_sgemm(f, c->sms, c->stream), "ffma sgemm");
+    }
+    Mat a{A, lda};
+    return run_chain(c, FG_DT_F32, FG_SEM_MATH, FG_F32_3XTF32, C, ldc, Mat{B, ldb}, N, 1, &a, &M, &K);
+}
+
+int host_sgemm(float *C, const float *A, const float *B, long M, long N, long K)
+{
+    if (M < 0 || N < 0 || K < 0) return fail(FG_ERR_INVALID, "negative dimension");
+    if (M == 0 || N == 0) return ok();
+    if (M > (1l << 30) || N > (1l << 30) || K > (1l << 30))
+        return fail(FG_ERR_INVALID, "dimension too large");
+    DevCtx *c;
+    int st;
+    if ((st = get_ctx(&c))) return st;
+    std::lock_guard<std::mutex> lk(c->mu);
+    const int algo = K == 0 ? FG_F32_FFMA : sgemm_algo();
+    const long ldk = round_up(K > 0 ? K : 1, 4), ldn = round_up(N, 4);
+    size_t need = carve_size((size_t)M * ldk * 4) + carve_size((size_t)K * ldn * 4) +
+                  carve_size((size_t)M * ldn * 4) + 4096;
+    if (algo == FG_F32_3XTF32) {
+        long Ms[1] = {M}, Ks[1] = {K};
+        need += chain_scratch(FG_DT_F32, algo, N, 1, Ms, Ks);
+    }
+    if ((st = arena_reserve(c, need))) return st;
+    float *ad = (float *)arena_take(c, (size_t)M * ldk * 4);
+    float *bd = (float *)arena_take(c, (size_t)(K > 0 ? K : 1) * ldn * 4);
+    float *cd = (float *)arena_take(c, (size_t)M * ldn * 4);
+    if (K > 0) {
+        CUDA_TRY(cudaMemcpy2DAsync(ad, ldk * 4, A, K * 4, K * 4, M, cudaMemcpyHostToDevice, c->stream));
+        CUDA_TRY(cudaMemcpy2DAsync(bd, ldn * 4, B, N * 4, N * 4, K, cudaMemcpyHostToDevice, c->stream));
+    }
+    // singlegemm blocks K by GEMM_K = 2048 and adds the partial sums into C
+    // (singlegemm/src/NN_mp.h:13, :247)
+    if ((st = run_sgemm(c, algo, cd, ldn, ad, ldk, bd, ldn, M, N, K, 2048))) return st;
+    CUDA_TRY(cudaMemcpy2DAsync(C, N * 4, cd, ldn * 4, N * 4, M, cudaMemcpyDeviceToHost, c->stream));
+    if ((st = collect_status(c))) return st;
+    return ok();
+}
+
+int g_shalom_threads = 24;
+
+// Order the library's stream after `user` on entry, and `user` after it on exit.
+// A null handle is CUDA's legacy default stream (the library's own stream is
+// non-blocking, so it is not ordered with the default stream implicitly).
+int fence_in(DevCtx *c, void *user)
+{
+    if (!user) user = (void *)cudaStreamLegacy;
+    CUDA_TRY(cudaEventRecord(c->ev_in, (cudaStream_t)user));
+    CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_in, 0));
+    return FG_OK;
+}
+int fence_out(DevCtx *c, void *user)
+{
+    if (!user) user = (void *)cudaStreamLegacy;
+    CUDA_TRY(cudaEventRecord(c->ev_out, c->stream));
+    CUDA_TRY(cudaStreamWaitEvent((cudaStream_t)user, c->ev_out, 0));
+    return FG_OK;
+}
+
+bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
+
+}  // namespace
+
+// ==================================================================== C ABI
+
+FG_EXPORT int flashgemm_thread_num = 1;
+
+FG_EXPORT void flashgemm_set_thread_num(int num) { flashgemm_thread_num = num; }
+
+FG_EXPORT void flashgemm_multi_f32f32f32(float *C, float *B, long N, int num_gemm, ...)
+{
+    va_list ap;
+    va_start(ap, num_gemm);
+    chain_va(FG_DT_F32, C, B, N, num_gemm, ap);
+    va_end(ap);
+}
+
+FG_EXPORT void flashgemm_multi_bf16bf16f32(float *C, uint16_t *B, long N, int num_gemm, ...)
+{
+    va_list ap;
+    va_start(ap, num_gemm);
+    chain_va(FG_DT_BF16, C, B, N, num_gemm, ap);
+    va_end(ap);
+}
+
+FG_EXPORT void flashgemm_multi_int8uint8int32(int *C, uint8_t *B, long N, int num_gemm, ...)
+{
+    va_list ap;
+    va_start(ap, num_gemm);
+    chain_va(FG_DT_INT8, C, B, N, num_gemm, ap);
+    va_end(ap);
+}
+
+FG_EXPORT void LibShalom_sgemm_mp(int transa, int transb, float *C, float *A, float *B, long M,
+                                  long N, long K)
+{
+    (void)transa;
+    if (transb == 1) {  // NT: the reference only picks a thread grid (FP32_ID23.c:39-43)
+        ok();
+        return;
+    }
+    if (transb != 0) {
+        fail(FG_ERR_INVALID, "transb must be 0 or 1");
+        return;
+    }
+    host_sgemm(C, A, B, M, N, K);
+}
+
+FG_EXPORT void LibShalom_set_thread_nums(int num) { g_shalom_threads = num; }
+
+FG_EXPORT void Small_NGM_NN_SGEMM(float *C, float *A, float *B, long M, long N, long K, int NUM,
+                                  int Tm, int Tn)
+{
+    (void)NUM; (void)Tm; (void)Tn;
+    host_sgemm(C, A, B, M, N, K);
+}
+
+FG_EXPORT void Small_MGN_NN_SGEMM(float *C, float *A, float *B, long M, long N, long K, int NUM,
+                                  int Tm, int Tn)
+{
+    (void)NUM; (void)Tm; (void)Tn;
+    host_sgemm(C, A, B, M, N, K);
+}
+
+// C++-linkage (mangled) names of the singlegemm entry points, which is how the
+// reference's g++-compiled callers reference them (singlegemm/FP32_ID23.c:35,
+// set_TmTn.h:61, NN_mp.h:11 and :245).
+#define FG_CXX_ALIAS(decl, mangled) __attribute__((visibility("default"))) decl __asm__(mangled)
+FG_CXX_ALIAS(void fg_cxx_sgemm_mp(int, int, float *, float *, float *, long, long, long),
+             "_Z18LibShalom_sgemm_mpiiPfS_S_lll");
+FG_CXX_ALIAS(void fg_cxx_set_thread_nums(int), "_Z25LibShalom_set_thread_numsi");
+FG_CXX_ALIAS(void fg_cxx_ngm(float *, float *, float *, long, long, long, int, int, int),
+             "_Z18Small_NGM_NN_SGEMMPfS_S_llliii");
+FG_CXX_ALIAS(void fg_cxx_mgn(float *, float *, float *, long, long, long, int, int, int),
+             "_Z18Small_MGN_NN_SGEMMPfS_S_llliii");
+void fg_cxx_sgemm_mp(int ta, int tb, float *C, float *A, float *B, long M, long N, long K)
+{
+    LibShalom_sgemm_mp(ta, tb, C, A, B, M, N, K);
+}
+void fg_cxx_set_thread_nums(int n) { LibShalom_set_thread_nums(n); }
+void fg_cxx_ngm(float *C, float *A, float *B, long M, long N, long K, int u, int tm, int tn)
+{
+    Small_NGM_NN_SGEMM(C, A, B, M, N, K, u, tm, tn);
+}
+void fg_cxx_mgn(float *C, float *A, float *B, long M, long N, long K, int u, int tm, int tn)
+{
+    Small_MGN_NN_SGEMM(C, A, B, M, N, K, u, tm, tn);
+}
+
+FG_EXPORT int fg_last_status(void) { return t_status; }
+FG_EXPORT const char *fg_last_error(void) { return t_msg; }
+FG_EXPORT void fg_set_semantics(int sem) { g_sem.store(sem == FG_SEM_MATH ? FG_SEM_MATH : FG_SEM_REF); }
+FG_EXPORT int fg_get_semantics(void) { return semantics(); }
+FG_EXPORT void fg_set_f32_algo(int a) { g_f32.store(a == FG_F32_FFMA ? FG_F32_FFMA : FG_F32_3XTF32); }
+FG_EXPORT int fg_get_f32_algo(void) { return f32_algo(); }
+FG_EXPORT void fg_set_sgemm_algo(int a) { g_sgemm.store(a == FG_F32_3XTF32 ? FG_F32_3XTF32 : FG_F32_FFMA); }
+FG_EXPORT int fg_get_sgemm_algo(void) { return sgemm_algo(); }
+FG_EXPORT unsigned long long fg_kernel_launches(void) { return g_launches.load(); }
+FG_EXPORT const char *fg_version(void) { return "flashgemm-b200 0.1 (sm_100a)"; }
+
+FG_EXPORT int fg_chain_dev(int dtype, void *C, const void *B, long N, int num_gemm,
+                           const void *const *A, const long *M, const long *K, void *stream)
+{
+    if (dtype != FG_DT_F32 && dtype != FG_DT_BF16 && dtype != FG_DT_INT8)
+        return fail(FG_ERR_INVALID, "unknown dtype %d", dtype);
+    if (!C || !B || !A || !M || !K) return fail(FG_ERR_INVALID, "null pointer");
+    int st = check_shapes(dtype, N, num_gemm, M, K);
+    if (st) return st;
+    for (int i = 0; i < num_gemm; ++i)
+        if (K[i] % 2 != 0) return fail(FG_ERR_INVALID, "gemm %d: K must be a multiple of 2", i + 1);
+    if (N == 0) return ok();
+    const int elt = elt_of(dtype);
+    if (!aligned16(C) || !aligned16(B))
+        return fail(FG_ERR_INVALID, "device pointers must be 16-byte aligned");
+    for (int i = 0; i < num_gemm; ++i)
+        if (!A[i]) return fail(FG_ERR_INVALID, "null weight pointer");
+    DevCtx *c;
+    if ((st = get_ctx(&c))) return st;
+    std::lock_guard<std::mutex> lk(c->mu);
+    const int algo = f32_algo();
+    const long ldN = round_up(N, 16);
+    // B needs 16-byte rows for the tensor path; otherwise it is staged padded
+    const bool tensor = !(dtype == FG_DT_F32 && algo == FG_F32_FFMA);
+    const bool pad_b = tensor && ((N * elt) % 16 != 0);
+    size_t need = chain_scratch(dtype, algo, N, num_gemm, M, K) + 4096;
+    if (pad_b) need += carve_size((size_t)K[0] * ldN * elt);
+    if ((st = arena_reserve(c, need))) return st;
+    if ((st = fence_in(c, stream))) return st;
+    Mat b{B, N};
+    if (pad_b) {
+        void *p = arena_take(c, (size_t)K[0] * ldN * elt);
+        CUDA_TRY(cudaMemcpy2DAsync(p, ldN * elt, B, N * elt, N * elt, K[0], cudaMemcpyDeviceToDevice,
+                                   c->stream));
+        b = Mat{p, ldN};
+    }
+    std::vector<Mat> a(num_gemm);
+    for (int i = 0; i < num_gemm; ++i) a[i] = Mat{A[i], K[i]};
+    if ((st = run_chain(c, dtype, semantics(), algo, C, N, b, N, num_gemm, a.data(), M, K)))
+        return st;
+    if ((st = fence_out(c, stream))) return st;
+    return ok();
+}
+
+FG_EXPORT int fg_sgemm_dev(float *C, const float *A, const float *B, long M, long N, long K,
+                           int algo, void *stream)
+{
+    if (!C || !A || !B) return fail(FG_ERR_INVALID, "null pointer");
+    if (M < 0 || N < 0 || K < 0) return fail(FG_ERR_INVALID, "negative dimension");
+    if (M == 0 || N == 0) return ok();
+    if (algo != FG_F32_FFMA && algo != FG_F32_3XTF32) return fail(FG_ERR_INVALID, "unknown algo");
+    if (algo == FG_F32_3XTF32 && (K == 0 || (N % 4) || !aligned16(B) || !aligned16(C)))
+        return fail(FG_ERR_UNSUPPORTED, "3xTF32 needs K > 0, N %% 4 == 0 and 16-byte-aligned B, C");
+    DevCtx *c;
+    int st;
+    if ((st = get_ctx(&c))) return st;
+    std::lock_guard<std::mutex> lk(c->mu);
+    size_t need = 4096;
+    if (algo == FG_F32_3XTF32) {
+        long Ms[1] = {M}, Ks[1] = {K};
+        need += chain_scratch(FG_DT_F32, algo, N, 1, Ms, Ks);
+    }
+    if ((st = arena_reserve(c, need))) return st;
+    if ((st = fence_in(c, stream))) return st;
+    if ((st = run_sgemm(c, algo, C, N, A, K, B, N, M, N, K, 2048))) return st;
+    if ((st = fence_out(c, stream))) return st;
+    return ok();
+}
+
+FG_EXPORT int fg_sync(void)
+{
+    DevCtx *c;
+    int st;
+    if ((st = get_ctx(&c))) return st;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if ((st = collect_status(c))) return st;
+    return ok();
+}

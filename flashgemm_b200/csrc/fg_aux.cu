@@ -1,0 +1,100 @@
+// Bandwidth-bound helper kernels around the GEMM stages: the FP32 -> TF32
+// hi/lo split that feeds 3xTF32 stages, and the INT8 weight preparation that
+// carries the reference's tail-row behaviour into the tensor-core path.
+#include <cuda_runtime.h>
+
+#include "fg_kernels.h"
+
+namespace fg {
+
+__device__ __forceinline__ float tf32_rne(float f)
+{
+    uint32_t u = __float_as_uint(f);
+    if ((u & 0x7f800000u) == 0x7f800000u) return f;
+    u += 0xfffu + ((u >> 13) & 1u);
+    return __uint_as_float(u & 0xffffe000u);
+}
+
+// x = hi + lo + r with hi = rne_tf32(x), lo = rne_tf32(x - hi), |r| <= 2^-22 |x|.
+__global__ void split_tf32_kernel(const float *__restrict__ in, long ld_in, float *__restrict__ hi,
+                                  float *__restrict__ lo, long ld_out, long rows, long cols)
+{
+    const long total = rows * cols;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+         i += (long)gridDim.x * blockDim.x) {
+        const long r = i / cols, c = i - r * cols;
+        const float x = in[r * ld_in + c];
+        const float h = tf32_rne(x);
+        hi[r * ld_out + c] = h;
+        lo[r * ld_out + c] = tf32_rne(x - h);
+    }
+}
+
+cudaError_t launch_split_tf32(const float *in, long ld_in, float *hi, float *lo, long ld_out,
+                              long rows, long cols, cudaStream_t s)
+{
+    if (rows <= 0 || cols <= 0) return cudaSuccess;
+    const long total = rows * cols;
+    long blocks = (total + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    split_tf32_kernel<<<(unsigned)blocks, 256, 0, s>>>(in, ld_in, hi, lo, ld_out, rows, cols);
+    return cudaGetLastError();
+}
+
+// Rows m in [tail_lo, tail_hi) of the reference's INT8 chain meet activation
+// k-quad max(s-1, 0) with weight k-quad s (multigemm/src/kernel_int8.h:405 vs
+// :427, :590 vs :608). The prepared copy shifts those rows left by one quad,
+// so a plain MMA yields sum_{s>=1} A_q(s) X_q(s-1); the missing A_q(0) X_q(0)
+// term is added by the GEMM epilogue from the first quad kept at [K, K + 4).
+// Other rows are copied unchanged; columns [K, ld_out) of them are zero.
+__global__ void prep_int8_weights_kernel(const int8_t *__restrict__ src, long ld_in,
+                                         uint8_t *__restrict__ dst, long ld_out, long M, long K,
+                                         long tail_lo, long tail_hi)
+{
+    const long total = M * ld_out;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+         i += (long)gridDim.x * blockDim.x) {
+        const long m = i / ld_out, k = i - m * ld_out;
+        const uint8_t *row = reinterpret_cast<const uint8_t *>(src) + m * ld_in;
+        uint8_t v = 0;
+        if (m >= tail_lo && m < tail_hi) {
+            if (k < K - 4)
+                v = row[k + 4];
+            else if (k >= K && k < K + 4)
+                v = row[k - K];
+        } else if (k < K) {
+            v = row[k];
+        }
+        dst[i] = v;
+    }
+}
+
+cudaError_t launch_prep_int8_weights(const int8_t *src, long ld_in, uint8_t *dst, long ld_out,
+                                     long M, long K, long tail_lo, long tail_hi, cudaStream_t s)
+{
+    if (M <= 0) return cudaSuccess;
+    const long total = M * ld_out;
+    long blocks = (total + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    prep_int8_weights_kernel<<<(unsigned)blocks, 256, 0, s>>>(src, ld_in, dst, ld_out, M, K,
+                                                               tail_lo, tail_hi);
+    return cudaGetLastError();
+}
+
+__global__ void fill_u32_kernel(uint32_t *dst, size_t count, uint32_t value)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
+         i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = value;
+}
+
+cudaError_t launch_fill_u32(uint32_t *dst, size_t count, uint32_t value, cudaStream_t s)
+{
+    if (count == 0) return cudaSuccess;
+    size_t blocks = (count + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    fill_u32_kernel<<<(unsigned)blocks, 256, 0, s>>>(dst, count, value);
+    return cudaGetLastError();
+}
+
+}  // namespace fg

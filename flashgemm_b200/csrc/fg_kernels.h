@@ -1,0 +1,70 @@
+// Internal interface between the host shim (fg_api.cpp) and the CUDA kernels.
+// Not installed; the public C ABI is in include/.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fg {
+
+// How a tensor-core GEMM stage writes its result.
+enum EpiKind : int {
+    EPI_F32 = 0,       // final stage, FP32 C (BF16 / TF32 chains, SGEMM)
+    EPI_S32 = 1,       // final stage, int32 C (INT8 chain)
+    EPI_BF16 = 2,      // between stages: FP32 -> BF16 (RNE), optional panel permutation
+    EPI_S8 = 3,        // between stages: int32 -> int8 (saturate), optional panel permutation
+    EPI_TF32SPLIT = 4  // between stages: FP32 -> (hi, lo) TF32 pair for the next 3xTF32 stage
+};
+
+enum OperandKind : int { OP_BF16 = 0, OP_I8 = 1, OP_TF32X3 = 2 };
+
+// One GEMM stage D[M x N] = W[M x K] * X[K x N]; W row-major with leading
+// dimension ld_w, X row-major with leading dimension ld_x (both in elements).
+struct StageArgs {
+    int op;            // OperandKind
+    int M, N, K;
+    const void *w;     // weights (TF32X3: hi part)
+    const void *w_lo;  // TF32X3: lo part (same ld)
+    long ld_w;
+    const void *x;     // activations (TF32X3: hi part)
+    const void *x_lo;  // TF32X3: lo part (same ld)
+    long ld_x;
+    int epi;           // EpiKind
+    void *out;         // C, or the next stage's activations (TF32SPLIT: hi)
+    void *out_lo;      // TF32SPLIT: lo
+    long ld_out;
+    int permute;       // 1: apply the reference's panel permutation (EPI_BF16 / EPI_S8)
+    int m_written;     // rows >= m_written are not stored (INT8 reference semantics)
+    int tail_lo;       // INT8 reference tail rows [tail_lo, tail_hi): weights pre-shifted,
+    int tail_hi;       //   first k-quad kept at w[m * ld_w + K .. +3], added in the epilogue
+    int *status;       // device status word (0 = ok)
+};
+
+cudaError_t launch_tc_stage(const StageArgs &a, int num_sms, cudaStream_t s);
+
+// Plain FP32 SGEMM on CUDA cores: C = A * B, one FMA per k in increasing k;
+// with kblock > 0 each block of kblock k is summed from zero and added to C.
+struct FfmaArgs {
+    int M, N, K;
+    const float *A; long lda;
+    const float *B; long ldb;
+    float *C; long ldc;
+    int kblock;
+};
+cudaError_t launch_ffma_sgemm(const FfmaArgs &a, int num_sms, cudaStream_t s);
+
+// FP32 -> (hi, lo) TF32 split of a rows x cols matrix (leading dims ld_in / ld_out).
+cudaError_t launch_split_tf32(const float *in, long ld_in, float *hi, float *lo, long ld_out,
+                              long rows, long cols, cudaStream_t s);
+
+// INT8 reference-semantics weight preparation: copies W (M x K, ld_in) into
+// dst (ld_out >= K + 4), shifting rows [tail_lo, tail_hi) left by one k-quad
+// (zero-filling the last quad) and keeping their first quad at [K, K + 4).
+cudaError_t launch_prep_int8_weights(const int8_t *src, long ld_in, uint8_t *dst, long ld_out,
+                                     long M, long K, long tail_lo, long tail_hi,
+                                     cudaStream_t s);
+
+// Copy of a rows x cols byte matrix between leading dimensions (device to device).
+cudaError_t launch_fill_u32(uint32_t *dst, size_t count, uint32_t value, cudaStream_t s);
+
+}  // namespace fg

@@ -1,0 +1,101 @@
+"""The C-ABI library on a machine without a GPU: it loads, exports every symbol
+the public headers declare (C names and the C++ names of the singlegemm entry
+points), and its host-side argument checks behave like the reference's."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+INC = os.path.join(ROOT, "include")
+
+
+@pytest.fixture(scope="module")
+def fg():
+    import flashgemm_b200 as fg
+    from flashgemm_b200 import build
+    build.build()
+    fg.lib()
+    return fg
+
+
+def declared_symbols():
+    names = set()
+    for h in os.listdir(INC):
+        text = open(os.path.join(INC, h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:extern\s+)?[A-Za-z_][\w\s\*]*?\b(\w+)\s*\(", text, re.M):
+            if m.group(1) not in ("if", "while", "return", "defined"):
+                names.add(m.group(1))
+        for m in re.finditer(r"^extern\s+int\s+(\w+)\s*;", text, re.M):
+            names.add(m.group(1))
+    return names
+
+
+def exported_symbols(path):
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True,
+                         check=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if line.strip()}
+
+
+def test_every_declared_symbol_is_exported(fg):
+    decl = declared_symbols()
+    # the reference's public API (multigemm/src/flashgemm.h:17-25, singlegemm entry points)
+    for must in ["flashgemm_thread_num", "flashgemm_set_thread_num", "flashgemm_multi_f32f32f32",
+                 "flashgemm_multi_bf16bf16f32", "flashgemm_multi_int8uint8int32",
+                 "LibShalom_sgemm_mp", "LibShalom_set_thread_nums", "Small_NGM_NN_SGEMM",
+                 "Small_MGN_NN_SGEMM", "fg_chain_dev", "fg_sgemm_dev", "fg_last_error"]:
+        assert must in decl, must
+    exported = exported_symbols(fg.LIB_PATH)
+    missing = sorted(decl - exported)
+    assert not missing, missing
+
+
+def test_cxx_linkage_names_are_exported(fg):
+    exported = exported_symbols(fg.LIB_PATH)
+    for mangled in ["_Z18LibShalom_sgemm_mpiiPfS_S_lll", "_Z25LibShalom_set_thread_numsi",
+                    "_Z18Small_NGM_NN_SGEMMPfS_S_llliii", "_Z18Small_MGN_NN_SGEMMPfS_S_llliii"]:
+        assert mangled in exported, mangled
+
+
+def test_library_needs_no_libcuda_to_load(fg):
+    out = subprocess.run(["ldd", fg.LIB_PATH], capture_output=True, text=True).stdout
+    assert "libcuda.so" not in out
+
+
+def test_thread_num_knob(fg):
+    fg.flashgemm_set_thread_num(8)
+    assert fg.flashgemm_thread_num() == 8
+    fg.flashgemm_set_thread_num(1)
+    assert fg.flashgemm_thread_num() == 1
+
+
+def test_odd_k_rejected_before_any_device_work(fg, capfd):
+    """flashgemm.c:13-22: K % 2 != 0 prints and returns, C untouched."""
+    B = np.zeros((63, 32), np.float32)
+    A = np.zeros((16, 63), np.float32)
+    C = np.full((16, 32), 5.0, np.float32)
+    fg.flashgemm_multi_f32f32f32(C, B, 32, 1, A, 16, 63)
+    assert "K must be a multiple of 2" in capfd.readouterr().out
+    assert fg.last_status() == fg.FG_ERR_INVALID
+    assert (C == 5.0).all()
+
+
+def test_shape_mismatch_rejected(fg):
+    B = np.zeros((64, 32), np.uint8)
+    A1 = np.zeros((16, 64), np.int8)
+    A2 = np.zeros((16, 18), np.int8)
+    C = np.zeros((16, 32), np.int32)
+    fg.flashgemm_multi_int8uint8int32(C, B, 32, 2, A1, 16, 64, A2, 16, 18)
+    assert fg.last_status() == fg.FG_ERR_INVALID
+    assert "previous M" in fg.last_error()
+
+
+def test_settings_round_trip(fg):
+    fg.set_semantics("math")
+    assert fg.get_semantics() == fg.FG_SEM_MATH
+    fg.set_semantics("ref")
+    assert fg.get_semantics() == fg.FG_SEM_REF
+    assert "sm_100a" in fg.version()

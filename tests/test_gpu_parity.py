@@ -1,0 +1,280 @@
+"""Parity of the B200 path with the reference, through the C ABI.
+
+Every computation here goes through libflashgemm_b200.so's reference-named
+entry points (flashgemm_multi_*, LibShalom_sgemm_mp) or its device entry
+points, and is checked against the oracle: the committed golden vectors the
+reference produced, the C restatement of the reference (bit-exact with it), and
+an FP64 evaluation for accuracy statements.
+
+Tolerances (stated per dtype, as in the contract for this path):
+  INT8  bit-exact against the reference semantics;
+  BF16  relative Frobenius error <= 1e-2 against the reference semantics
+        (observed ~1e-3: FP32 accumulation order differs from vdpbf16ps, which
+        flips a few BF16 roundings between stages);
+  FP32  plain-FMA kernel bit-exact; 3xTF32 within 2x the plain kernel's own
+        error against FP64.
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+BF16_TOL = 1e-2
+
+
+@pytest.fixture(scope="module", autouse=True)
+def fg():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import flashgemm_b200 as fg
+    fg.lib()
+    fg.set_semantics("ref")
+    fg.set_f32_algo("3xtf32")
+    fg.set_sgemm_algo("ffma")
+    fg.flashgemm_set_thread_num(1)
+    yield fg
+    fg.set_semantics("ref")
+    fg.set_f32_algo("3xtf32")
+    fg.set_sgemm_algo("ffma")
+    fg.flashgemm_set_thread_num(1)
+
+
+def run_chain(fg, dt, B, As, N, Ms, Ks, C=None, threads=1):
+    fg.flashgemm_set_thread_num(threads)
+    if C is None:
+        C = np.zeros((Ms[-1], N), np.int32 if dt == "int8" else np.float32)
+    trip = []
+    for A, m, k in zip(As, Ms, Ks):
+        trip += [A, m, k]
+    fn = {"f32": fg.flashgemm_multi_f32f32f32, "bf16": fg.flashgemm_multi_bf16bf16f32,
+          "int8": fg.flashgemm_multi_int8uint8int32}[dt]
+    fn(C, B, N, len(As), *trip, check=True)
+    return C
+
+
+def assert_parity(dt, got, want, rows=None):
+    if rows is not None:
+        got, want = got[:rows], want[:rows]
+    if dt == "int8":
+        np.testing.assert_array_equal(got, want)
+    else:
+        err = oracle.rel_frob(got, want)
+        assert err <= BF16_TOL if dt == "bf16" else err <= 1e-5, err
+
+
+# ---------------------------------------------------------------- single stages (MATH)
+
+@pytest.mark.parametrize("dt", ["int8", "bf16", "f32"])
+@pytest.mark.parametrize("shape", [(128, 256, 128), (200, 96, 64), (64, 512, 256), (300, 520, 96)])
+def test_single_stage_matches_oracle(fg, dt, shape):
+    M, N, K = shape
+    B, As, Ks = oracle.chain_inputs(dt, N, K, [M], seed=M + N)
+    fg.set_semantics("math")
+    try:
+        got = run_chain(fg, dt, B, As, N, [M], Ks)
+    finally:
+        fg.set_semantics("ref")
+    if dt == "f32":
+        want = oracle.chain_f64(B, As, N, [M], Ks)
+        assert oracle.rel_frob(got, want) < 2e-6
+    else:
+        want = oracle.chain(dt, B, As, N, [M], Ks, mode=oracle.MATH)
+        assert_parity(dt, got, want)
+
+
+# ---------------------------------------------------------------- golden vectors
+
+def _golden(name):
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    return {k: z[k] for k in z.files}
+
+
+@pytest.mark.parametrize("name", ["int8_chain_3stage", "int8_chain_tails", "int8_chain_c3_widths",
+                                  "int8_chain_unwritten_rows", "bf16_chain_3stage",
+                                  "bf16_chain_tails", "f32_chain_n96"])
+def test_chain_matches_reference_golden(fg, name):
+    g = _golden(name)
+    dt = str(g["dtype"])
+    Ms = [int(x) for x in g["Ms"]]
+    Ks = [int(x) for x in g["Ks"]]
+    B = g["B"]
+    As = [g[f"A{i}"] for i in range(len(Ms))]
+    N = int(g["N"])
+    C = np.zeros_like(g["C"])
+    if dt == "int8":
+        C[:] = int(g["sentinel"])  # rows the reference never writes must stay untouched
+    got = run_chain(fg, dt, B, As, N, Ms, Ks, C=C, threads=int(g["threads"]))
+    if dt == "f32":
+        want64 = oracle.chain_f64(B, As, N, Ms, Ks)
+        e_ref = oracle.rel_frob(g["C"], want64)
+        assert oracle.rel_frob(got, want64) <= 2 * e_ref + 1e-7
+    else:
+        assert_parity(dt, got, g["C"])
+
+
+@pytest.mark.parametrize("name", ["f32_sgemm_96x128x64", "f32_sgemm_ksplit_48x128x2080",
+                                  "f32_sgemm_mgn_768x64x96"])
+def test_sgemm_matches_reference_golden_bitexact(fg, name):
+    g = _golden(name)
+    M, N, K = int(g["M"]), int(g["N"]), int(g["K"])
+    if "A" in g:
+        A, B = g["A"], g["B"]
+    else:
+        A, B = oracle.sgemm_inputs(M, N, K, int(g["seed"]))
+    C = np.zeros((M, N), np.float32)
+    fg.LibShalom_sgemm_mp(0, 0, C, A, B, M, N, K, check=True)
+    np.testing.assert_array_equal(C, g["C"])
+
+
+# ---------------------------------------------------------------- seeded sweeps
+
+CHAIN_SHAPES = [
+    # N, K1, Ms        (M % 12 in {0, 4, 8}, several M and N tiles, K not a multiple of 128)
+    (256, 64, [48, 96, 24]),
+    (512, 128, [40, 20, 16]),
+    (320, 96, [36, 28, 32]),
+    (544, 256, [136, 260, 100, 44]),
+    (1024, 512, [384, 128, 256]),
+    (96, 32, [12, 24]),
+]
+
+
+@pytest.mark.parametrize("dt", ["int8", "bf16"])
+@pytest.mark.parametrize("shape", CHAIN_SHAPES)
+def test_chain_matches_oracle_ref_semantics(fg, dt, shape):
+    N, K1, Ms = shape
+    B, As, Ks = oracle.chain_inputs(dt, N, K1, Ms, seed=len(Ms) * 1000 + N)
+    want = oracle.chain(dt, B, As, N, Ms, Ks, mode=oracle.REF, threads=1)
+    got = run_chain(fg, dt, B, As, N, Ms, Ks)
+    rows = (Ms[-1] // 4) * 4 if dt == "int8" else None
+    assert_parity(dt, got, want, rows)
+
+
+@pytest.mark.parametrize("dt", ["int8", "bf16"])
+@pytest.mark.parametrize("shape", CHAIN_SHAPES[:4])
+def test_chain_math_semantics(fg, dt, shape):
+    N, K1, Ms = shape
+    B, As, Ks = oracle.chain_inputs(dt, N, K1, Ms, seed=7 + N)
+    fg.set_semantics("math")
+    try:
+        got = run_chain(fg, dt, B, As, N, Ms, Ks)
+    finally:
+        fg.set_semantics("ref")
+    want = oracle.chain(dt, B, As, N, Ms, Ks, mode=oracle.MATH)
+    assert_parity(dt, got, want)
+    if dt == "bf16":
+        Bf = oracle.bf16_to_f32(B)
+        Af = [oracle.bf16_to_f32(a) for a in As]
+        assert oracle.rel_frob(got, oracle.chain_f64(Bf, Af, N, Ms, Ks)) < BF16_TOL
+
+
+@pytest.mark.parametrize("shape", [(256, 64, [48, 96, 24]), (520, 100, [130, 66]),
+                                   (100, 64, [40, 24])])
+def test_f32_chain_ffma_bitexact_and_3xtf32_accuracy(fg, shape):
+    N, K1, Ms = shape
+    B, As, Ks = oracle.chain_inputs("f32", N, K1, Ms, seed=N)
+    want32 = oracle.chain("f32", B, As, N, Ms, Ks)
+    want64 = oracle.chain_f64(B, As, N, Ms, Ks)
+    fg.set_f32_algo("ffma")
+    try:
+        ffma = run_chain(fg, "f32", B, As, N, Ms, Ks)
+    finally:
+        fg.set_f32_algo("3xtf32")
+    np.testing.assert_array_equal(ffma, want32)
+    tf = run_chain(fg, "f32", B, As, N, Ms, Ks)
+    e_ffma = oracle.rel_frob(ffma, want64)
+    e_tf = oracle.rel_frob(tf, want64)
+    assert e_tf <= 2 * e_ffma, (e_tf, e_ffma)
+
+
+@pytest.mark.parametrize("shape", [(1024, 1024, 1024), (128, 2048, 4096), (512, 64, 128),
+                                   (777, 333, 129)])
+def test_sgemm_ffma_bitexact_and_3xtf32(fg, shape):
+    M, N, K = shape
+    A, B = oracle.sgemm_inputs(M, N, K, seed=M)
+    want = oracle.sgemm_f32(A, B, kblock=2048)
+    C = np.zeros((M, N), np.float32)
+    fg.LibShalom_sgemm_mp(0, 0, C, A, B, M, N, K, check=True)
+    np.testing.assert_array_equal(C, want)
+    want64 = oracle.sgemm_f64(A, B)
+    fg.set_sgemm_algo("3xtf32")
+    try:
+        C2 = np.zeros((M, N), np.float32)
+        fg.LibShalom_sgemm_mp(0, 0, C2, A, B, M, N, K, check=True)
+    finally:
+        fg.set_sgemm_algo("ffma")
+    assert oracle.rel_frob(C2, want64) <= 2 * oracle.rel_frob(C, want64)
+
+
+def test_sgemm_nt_mode_leaves_c_untouched(fg):
+    A, B = oracle.sgemm_inputs(64, 64, 64, seed=1)
+    C = np.full((64, 64), 3.0, np.float32)
+    fg.LibShalom_sgemm_mp(0, 1, C, A, B, 64, 64, 64, check=True)
+    assert (C == 3.0).all()
+
+
+# ---------------------------------------------------------------- full sizes (sampled panels)
+
+def _panel_cols(N, panels):
+    return np.concatenate([np.arange(32 * p, 32 * p + 32) for p in panels])
+
+
+@pytest.mark.parametrize("dt,N,K1,Ms", [
+    ("bf16", 4096, 1024, [4096, 1024, 1024]),             # BF16 chain of 3 GEMMs
+    ("int8", 8192, 2048, [4096, 2048, 4096, 1024]),       # INT8 chain of 4 GEMMs
+])
+def test_full_size_chain_on_sampled_panels(fg, dt, N, K1, Ms):
+    """The reference's permutation stays inside 32-column panels, so panel p of C
+    depends only on panel p of B: full-size results are checked exactly on a
+    sample of panels by running the oracle on just those columns."""
+    B, As, Ks = oracle.chain_inputs(dt, N, K1, Ms, seed=2024)
+    got = run_chain(fg, dt, B, As, N, Ms, Ks)
+    panels = [0, 1, N // 64, N // 32 - 1]
+    cols = _panel_cols(N, panels)
+    Bs = np.ascontiguousarray(B[:, cols])
+    want = oracle.chain(dt, Bs, As, len(cols), Ms, Ks, mode=oracle.REF, threads=1)
+    rows = (Ms[-1] // 4) * 4 if dt == "int8" else None
+    assert_parity(dt, np.ascontiguousarray(got[:, cols]), want, rows)
+    if dt == "int8":
+        # every stage saturates at these widths: the output is bounded by K * 255 * 128
+        assert np.abs(got.astype(np.int64)).max() <= Ks[-1] * 255 * 128
+
+
+# ---------------------------------------------------------------- device entry points
+
+@pytest.mark.parametrize("dt", ["int8", "bf16", "f32"])
+def test_device_api_matches_host_api(fg, dt):
+    import torch
+    N, K1, Ms = 512, 128, [256, 96, 64]
+    B, As, Ks = oracle.chain_inputs(dt, N, K1, Ms, seed=99)
+    host = run_chain(fg, dt, B, As, N, Ms, Ks)
+    tdt = {"int8": torch.int8, "bf16": torch.int16, "f32": torch.float32}[dt]
+    tB = torch.from_numpy(B.view(np.int8) if dt == "int8" else
+                          (B.view(np.int16) if dt == "bf16" else B)).cuda()
+    tA = [torch.from_numpy(a.view(np.int16) if dt == "bf16" else a).cuda() for a in As]
+    tC = torch.zeros((Ms[-1], N), dtype=torch.int32 if dt == "int8" else torch.float32,
+                     device="cuda")
+    fg.chain_dev(dt, tC, tB, N, tA, Ms, Ks)
+    torch.cuda.synchronize()
+    fg.sync()
+    np.testing.assert_array_equal(tC.cpu().numpy(), host)
+    assert tdt is not None
+
+
+def test_odd_k_prints_and_returns_like_the_reference(fg, capfd):
+    B, As, Ks = oracle.chain_inputs("f32", 64, 63, [32], seed=1)
+    C = np.full((32, 64), 7.0, np.float32)
+    fg.flashgemm_multi_f32f32f32(C, B, 64, 1, As[0], 32, 63)
+    assert "K must be a multiple of 2" in capfd.readouterr().out
+    assert fg.last_status() == fg.FG_ERR_INVALID
+    assert (C == 7.0).all()
+
+
+def test_mismatched_chain_is_rejected(fg):
+    B, As, Ks = oracle.chain_inputs("int8", 64, 64, [32, 32], seed=1)
+    C = np.zeros((32, 64), np.int32)
+    fg.flashgemm_multi_int8uint8int32(C, B, 64, 2, As[0], 32, 64, As[1], 32, 48)
+    assert fg.last_status() == fg.FG_ERR_INVALID
