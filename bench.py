@@ -1,0 +1,442 @@
+"""Benchmark of the flashgemm hot path on B200: one JSON line on stdout.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload bf16-chain|int8-chain|f32-gemm]
+
+A step is one pass of the hot path over one batch: by default the BF16 chain
+of three GEMMs C = A3*(A2*(A1*B)) with B 1024 x 4096 (the activations X
+[4096 x 1024] of X*W1*W2*W3, in the reference's orientation) and weights
+4096 x 1024, 1024 x 4096, 1024 x 1024, BF16 inputs, FP32 accumulation, BF16
+intermediates with the reference's panel permutation, FP32 output. Inputs are
+seeded synthetic data in HBM; L2 is flushed (a 256 MiB write) between timed
+steps, outside each step's events.
+
+Multi-GPU (torchrun, one process per GPU): the activation columns are
+partitioned, so every rank runs its own full step on its own shard with no
+data-path collective (weak scaling); NCCL carries only the barrier and the
+max-over-ranks time.
+
+--impl reference times the reference's own CPU implementation (compiled from
+its sources into oracle/_ref) on this machine's host cores, on a bounded
+column sample of the same workload, and prints the same line with
+"impl": "reference".
+"""
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (dtype, N, K1, Ms)
+    "bf16-chain": ("bf16", 4096, 1024, [4096, 1024, 1024]),
+    "int8-chain": ("int8", 8192, 2048, [4096, 2048, 4096, 1024]),
+    "f32-gemm": ("f32", 1024, 1024, [1024]),
+}
+DESCR = {
+    "bf16-chain": "BF16 chain of 3 GEMMs: X[4096x1024]*W1[1024x4096]*W2[4096x1024]*W3[1024x1024]",
+    "int8-chain": "INT8 chain of 4 GEMMs: X[8192x2048]*W1..W4, widths 2048->4096->2048->4096->1024",
+    "f32-gemm": "single FP32 GEMM C=A*B, M=N=K=1024 (plain FP32 FMA kernel)",
+}
+
+
+def flops_of(N, K1, Ms):
+    Ks = [K1] + Ms[:-1]
+    return sum(2.0 * N * m * k for m, k in zip(Ms, Ks))
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p, "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, \
+            "fallback"
+
+
+# ---------------------------------------------------------------- clocks (NVML, read only)
+
+class ClockSampler:
+    """Samples SM clock and clock-event reasons of one GPU every 10 ms."""
+
+    REASONS = {
+        "gpu_idle": 0x1, "applications_clocks_setting": 0x2, "sw_power_cap": 0x4,
+        "hw_slowdown": 0x8, "sync_boost": 0x10, "sw_thermal_slowdown": 0x20,
+        "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80,
+    }
+
+    def __init__(self, index):
+        self.samples = []
+        self.reasons = 0
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._h = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception:  # noqa: BLE001 - clocks are reported as unavailable
+            self._h = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                mhz = self._nv.nvmlDeviceGetClockInfo(self._h, self._nv.NVML_CLOCK_SM)
+                r = self._nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                util = self._nv.nvmlDeviceGetUtilizationRates(self._h).gpu
+                self.samples.append((mhz, r, util))
+            except Exception:  # noqa: BLE001
+                pass
+            time.sleep(0.01)
+
+    def __enter__(self):
+        if self._h is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self._h is not None:
+            self._stop.set()
+            self._t.join()
+
+    def summary(self):
+        if self._h is None or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unavailable"]}
+        loaded = [s for s in self.samples if s[2] > 0] or self.samples
+        mhz = statistics.median(s[0] for s in loaded)
+        bits = 0
+        for s in loaded:
+            bits |= s[1]
+        names = [k for k, v in self.REASONS.items() if bits & v and k != "gpu_idle"]
+        return {"sm_mhz": mhz, "sm_max_mhz": self.max_mhz, "reasons": names,
+                "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- CPU reference / port
+
+def cpu_info():
+    flags = set()
+    model = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags") and not flags:
+                    flags = set(line.split(":", 1)[1].split())
+                if line.startswith("model name") and not model:
+                    model = line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return flags, model
+
+
+def reference_runner():
+    """The reference's own implementation if it was built here and this CPU
+    runs its instructions (AVX-512 F/BW, VNNI, BF16); else the C port."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    flags, model = cpu_info()
+    need = {"avx512f", "avx512bw", "avx512_vnni", "avx512_bf16"}
+    if oracle.ref_available() and need <= flags:
+        return oracle, "reference", model, "amx_tile" in flags
+    return oracle, "port", model, "amx_tile" in flags
+
+
+def time_cpu(workload, steps=None, warmup=1, budget_s=12.0):
+    """TFLOP/s of the reference (or port) on a column sample of the workload.
+
+    steps=None: repeat for about budget_s seconds (the cpu_baseline leg).
+    steps=K: exactly K timed steps, the column sample sized from one calibration
+    call so that the K steps take about a minute in total.
+    Returns (tflops, descr dict, per-step seconds)."""
+    oracle, kind, model, amx = reference_runner()
+    dt, N, K1, Ms = WORKLOADS[workload]
+    threads = os.cpu_count() or 1
+
+    def prepare(ns):
+        if dt == "f32":
+            A, Bm = oracle.sgemm_inputs(Ms[0], ns, K1, seed=1)
+
+            def one():
+                if kind == "reference":
+                    oracle.ref_sgemm(A, Bm, threads=threads)
+                else:
+                    oracle.sgemm_f32(A, Bm)
+        else:
+            B, As, Ks = oracle.chain_inputs(dt, ns, K1, Ms, seed=1)
+
+            def one():
+                if kind == "reference":
+                    oracle.ref_chain(dt, B, As, ns, Ms, Ks, threads=threads)
+                else:
+                    oracle.chain(dt, B, As, ns, Ms, Ks, mode=oracle.REF, threads=threads)
+        return one
+
+    ns = min(N, 512)
+    one = prepare(ns)
+    t0 = time.perf_counter()
+    one()
+    t_cal = time.perf_counter() - t0
+    if steps is not None:
+        per_step = 60.0 / max(steps + warmup, 1)
+        ns = int(ns * per_step / max(t_cal, 1e-6)) // 32 * 32
+        ns = max(32, min(N, ns))
+        one = prepare(ns)
+    for _ in range(warmup):
+        one()
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while True:
+        t0 = time.perf_counter()
+        one()
+        times.append(time.perf_counter() - t0)
+        if steps is not None:
+            if len(times) >= steps:
+                break
+        elif len(times) >= 3 and time.perf_counter() > t_end:
+            break
+    fl = flops_of(ns, K1, Ms)
+    med = statistics.median(times)
+    descr = {"kind": kind, "cores": threads, "cpu": model, "amx_available": amx,
+             "amx_used": False,
+             "sample": f"{ns} of {N} activation columns per step (work scales with columns), "
+                       f"median of {len(times)} steps"}
+    return fl / med / 1e12, descr, times
+
+
+# ---------------------------------------------------------------- GPU arm
+
+def make_inputs(dt, N, K1, Ms, seed):
+    """Seeded synthetic operands (host numpy), same distributions as the tests:
+    f32 U[-1, 1]; bf16 N(0,1)/sqrt(K) rounded to BF16; int8 U{-127..127}."""
+    rng = np.random.default_rng(seed)
+    Ks = [K1] + Ms[:-1]
+    if dt == "f32":
+        B = rng.uniform(-1, 1, (K1, N)).astype(np.float32)
+        As = [rng.uniform(-1, 1, (m, k)).astype(np.float32) for m, k in zip(Ms, Ks)]
+    elif dt == "bf16":
+        def bf(x):
+            u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+            return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+        B = bf(rng.standard_normal((K1, N)))
+        As = [bf(rng.standard_normal((m, k)) / np.sqrt(k)) for m, k in zip(Ms, Ks)]
+    else:
+        B = rng.integers(-127, 128, size=(K1, N)).astype(np.int8).view(np.uint8)
+        As = [rng.integers(-127, 128, size=(m, k)).astype(np.int8) for m, k in zip(Ms, Ks)]
+    return B, As, Ks
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="bf16-chain", choices=list(WORKLOADS))
+    ap.add_argument("--e2e-steps", type=int, default=None,
+                    help="steps of the host-buffer C-ABI measurement (default: min(steps, 200))")
+    ap.add_argument("--cpu-budget", type=float, default=12.0,
+                    help="seconds of reference CPU work for the cpu_baseline leg")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dt, N, K1, Ms = WORKLOADS[args.workload]
+    metric = {"f32": "FP32 GEMM TFLOP/s"}.get(dt, "fused GEMM-chain TFLOP/s")
+    config = {"workload": DESCR[args.workload], "dtype": dt, "N": N, "K1": K1, "M": Ms,
+              "gflop_per_step_per_gpu": flops_of(N, K1, Ms) / 1e9,
+              "semantics": "reference (panel permutation, INT8 tail rows)",
+              "l2": "flushed between steps (256 MiB write outside the step events)",
+              "parallelism": f"dp{world} (activation columns partitioned, no collective)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        tf, descr, times = time_cpu(args.workload, steps=args.steps, warmup=args.warmup)
+        line = {"impl": "reference", "metric": metric, "value": tf, "unit": "TFLOP/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * statistics.median(times), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": dt,
+                "data": "synthetic (seeded)", "config": config,
+                "cpu_baseline": dict(descr, value=tf, unit="TFLOP/s"),
+                "e2e": {"value": tf, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    import flashgemm_b200 as fg
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    dev = torch.device("cuda", local_rank)
+    fg.lib()
+    fg.set_semantics("ref")
+    fg.flashgemm_set_thread_num(1)
+
+    # --------------------------------------------------------- device-resident step
+    B, As, Ks = make_inputs(dt, N, K1, Ms, seed=1234 + rank)
+
+    def to_dev(a):
+        if a.dtype == np.uint16:
+            a = a.view(np.int16)
+        elif a.dtype == np.uint8:
+            a = a.view(np.int8)
+        return torch.from_numpy(a).to(dev)
+
+    tB = to_dev(B)
+    tA = [to_dev(a) for a in As]
+    tC = torch.empty((Ms[-1], N), dtype=torch.int32 if dt == "int8" else torch.float32,
+                     device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    if dt == "f32":
+        def step():
+            fg.sgemm_dev(tC, tA[0], tB, Ms[0], N, K1, "ffma")
+        kind = fg.FG_PK_FFMA
+    else:
+        def step():
+            fg.chain_dev(dt, tC, tB, N, tA, Ms, Ks)
+        kind = fg.FG_PK_TC_BF16 if dt == "bf16" else fg.FG_PK_TC_I8
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize(dev)
+    fg.sync()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    sampler = ClockSampler(torch.cuda.current_device() if world == 1 else local_rank)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    l0 = fg.kernel_launches()
+    fg.profile_begin()
+    with sampler:
+        t_wall = time.perf_counter()
+        for i in range(args.steps):
+            flush.fill_(i & 0xFF)
+            starts[i].record()
+            step()
+            stops[i].record()
+        torch.cuda.synchronize(dev)
+        fg.sync()
+        t_wall = time.perf_counter() - t_wall
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    fg.profile_end()
+    launches = fg.kernel_launches() - l0
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
+    total_ms = sum(step_ms)
+    k_ms, k_n, k_fl = fg.profile_query(kind)
+
+    # max over ranks
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    step_flops = flops_of(N, K1, Ms)
+    value = world * step_flops * args.steps / (total_ms / 1e3) / 1e12
+
+    # --------------------------------------------------------- end to end through the C ABI
+    e2e_steps = args.e2e_steps or min(args.steps, 200)
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+    hB = pin(B)
+    hA = [pin(a) for a in As]
+    hC = pin(np.zeros((Ms[-1], N), np.int32 if dt == "int8" else np.float32))
+    trip = []
+    for a, m, k in zip(hA, Ms, Ks):
+        trip += [a, m, k]
+    if dt == "f32":
+        def e2e_step():
+            fg.LibShalom_sgemm_mp(0, 0, hC, hA[0], hB, Ms[0], N, K1, check=True)
+    else:
+        fn = {"bf16": fg.flashgemm_multi_bf16bf16f32,
+              "int8": fg.flashgemm_multi_int8uint8int32}[dt]
+
+        def e2e_step():
+            fn(hC, hB, N, len(Ms), *trip, check=True)
+    for _ in range(3):
+        e2e_step()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * step_flops * e2e_steps / e2e_s / 1e12
+    h2d = hB.nbytes + sum(a.nbytes for a in hA)
+    d2h = hC.nbytes
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    peaks, peak_src = load_peaks()
+    achieved = k_fl / (k_ms / 1e3) / 1e12 if k_ms > 0 else None
+    if dt == "bf16":
+        peak, peak_name = peaks.get("bf16_tflops"), "bf16_tflops (cuBLAS BF16 burst, measured)"
+    elif dt == "int8":
+        # no INT8 measurement in the peaks file: the B200's dense INT8 rate is twice
+        # its BF16 rate per clock, so twice the measured BF16 figure stands in
+        peak = 2 * peaks.get("bf16_tflops")
+        peak_name = "2 x bf16_tflops (INT8 = 2x BF16 per clock; measured BF16)"
+    else:
+        sm_mhz = peaks.get("sm_max_mhz", 1965.0)
+        peak = 148 * 256 * sm_mhz * 1e6 / 1e12
+        peak_name = "148 SMs x 128 FFMA/clk x 2 x sm_max_mhz (datasheet-style FFMA peak)"
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            traffic = json.load(f).get(args.workload)
+    except (OSError, ValueError):
+        traffic = None
+    roofline = {"bound": "tensor" if dt != "f32" else "tensor", "achieved": achieved,
+                "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if achieved and peak else None,
+                "traffic": traffic.get("bytes_per_launch") if traffic else None,
+                "kernel": "fg::tc_stage_kernel" if dt != "f32" else "fg::ffma_sgemm_kernel",
+                "launches_timed": k_n, "avg_launch_us": 1e3 * k_ms / k_n if k_n else None,
+                "peak_source": f"{peak_name}; {peak_src}"}
+
+    line = {"metric": metric, "value": value, "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dt,
+            "data": "synthetic (seeded; no dataset involved)", "config": config,
+            "clocks": sampler.summary(), "gpu_launches": launches,
+            "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                    "api": "flashgemm_multi_*/LibShalom_sgemm_mp, pinned host buffers"},
+            "roofline": roofline, "wall_s_timed_region": t_wall}
+    if world == 1:
+        tf, descr, _ = time_cpu(args.workload, budget_s=args.cpu_budget)
+        line["cpu_baseline"] = dict(descr, value=tf, unit="TFLOP/s")
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -206,3 +206,48 @@ def sgemm_dev(C, A, B, M, N, K, algo="ffma", stream=None):
     st = lib().fg_sgemm_dev(C.data_ptr(), A.data_ptr(), B.data_ptr(), int(M), int(N), int(K), a, s)
     if st != FG_OK:
         raise FlashgemmError(st, last_error())
+
+
+# ------------------------------------------------------------ per-launch timing
+
+FG_PK_TC_BF16, FG_PK_TC_I8, FG_PK_TC_TF32X3, FG_PK_FFMA, FG_PK_AUX = range(5)
+
+
+def profile_begin():
+    st = lib().fg_profile_begin()
+    if st != FG_OK:
+        raise FlashgemmError(st, last_error())
+
+
+def profile_end():
+    lib().fg_profile_end()
+
+
+def profile_query(kind=-1):
+    """(device ms, launches, algorithmic FLOPs) of the kernels of one class
+    launched since profile_begin(); kind=-1 sums every class."""
+    ms = ctypes.c_double()
+    n = ctypes.c_ulonglong()
+    fl = ctypes.c_double()
+    st = lib().fg_profile_query(int(kind), ctypes.byref(ms), ctypes.byref(n), ctypes.byref(fl))
+    if st != FG_OK:
+        raise FlashgemmError(st, last_error())
+    return ms.value, int(n.value), fl.value
+
+
+# ------------------------------------------------------------ multi-GPU partitioning
+
+def shard_columns(N, world, rank, panel=32):
+    """Column range [start, stop) of the activations/outputs that `rank` of
+    `world` owns when one chain is split across GPUs. The chain is independent
+    per column except that the reference's between-stage permutation mixes the
+    columns of each 32-column panel, so shards are cut on panel boundaries:
+    each rank then runs the unchanged chain on its slice of B and writes its
+    slice of C, with no collective on the data path."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("bad world/rank")
+    panels = (N + panel - 1) // panel
+    per, extra = divmod(panels, world)
+    p0 = rank * per + min(rank, extra)
+    p1 = p0 + per + (1 if rank < extra else 0)
+    return min(p0 * panel, N), min(p1 * panel, N)

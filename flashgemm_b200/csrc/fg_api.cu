@@ -100,6 +100,23 @@ int sgemm_algo()
 
 inline long round_up(long x, long a) { return (x + a - 1) / a * a; }
 
+// 3xTF32: k-blocks of 32 between FP32 promotions of the tensor-core partial sum.
+// The tensor core's FP32 accumulation error grows with the number of MMAs that
+// feed one accumulator; promoting every block keeps small-K GEMMs below the
+// FFMA loop's own error, and longer chunks do the same for large K, where the
+// FFMA error is larger, at a smaller epilogue cost (measured on B200: error
+// ratio to FFMA <= 0.9 at K = 48..512 with 1 block, <= 0.5 at K >= 1024 with 3).
+// FG_TF32_CHUNK (k elements) overrides the choice.
+int tf32_chunk_blocks(long K)
+{
+    static const long forced = [] {
+        const char *v = getenv("FG_TF32_CHUNK");
+        return v ? atol(v) : 0l;
+    }();
+    if (forced > 0) return (int)((forced + 31) / 32);
+    return K <= 512 ? 1 : (K <= 2048 ? 2 : 3);
+}
+
 // ---------------------------------------------------------------- per-device context
 
 struct DevCtx {
@@ -113,7 +130,17 @@ struct DevCtx {
     size_t arena_off = 0;
     int *status = nullptr;       // device word the kernels report into
     int *status_host = nullptr;  // pinned copy
+    // per-launch device timing (fg_profile_begin / fg_profile_query)
+    struct Rec {
+        cudaEvent_t a, b;
+        int kind;
+        double flops;
+    };
+    std::vector<Rec> prof;       // records in use
+    std::vector<Rec> prof_pool;  // events to reuse
 };
+
+std::atomic<int> g_prof_on{0};
 
 std::mutex g_ctx_mu;
 DevCtx *g_ctx[64];
@@ -234,6 +261,35 @@ int launch(cudaError_t e, const char *what)
     return FG_OK;
 }
 
+// Launch one kernel through `fn`; while profiling is on, bracket it with CUDA
+// events on the library's stream (the stream the kernel runs on).
+template <class Fn>
+int run_kernel(DevCtx *c, int kind, double flops, const char *what, Fn &&fn)
+{
+    DevCtx::Rec r{nullptr, nullptr, kind, flops};
+    const bool prof = g_prof_on.load(std::memory_order_relaxed) != 0;
+    if (prof) {
+        if (!c->prof_pool.empty()) {
+            r.a = c->prof_pool.back().a;
+            r.b = c->prof_pool.back().b;
+            c->prof_pool.pop_back();
+        } else {
+            CUDA_TRY(cudaEventCreate(&r.a));
+            CUDA_TRY(cudaEventCreate(&r.b));
+        }
+        CUDA_TRY(cudaEventRecord(r.a, c->stream));
+    }
+    const int st = launch(fn(), what);
+    if (prof) {
+        CUDA_TRY(cudaEventRecord(r.b, c->stream));
+        c->prof.push_back(r);
+    }
+    return st;
+}
+
+int tc_kind(int op) { return op == OP_BF16 ? FG_PK_TC_BF16 : op == OP_I8 ? FG_PK_TC_I8 : FG_PK_TC_TF32X3; }
+double gemm_flops(long M, long N, long K) { return 2.0 * (double)M * (double)N * (double)K; }
+
 // Runs the chain on c->stream. Device operands: B (K[0] x N, ld b.ld),
 // A[i] (M[i] x K[i], ld a[i].ld, 16-byte-aligned rows where the tensor path
 // needs them), C (M[n-1] x N, ld ldc). Scratch must already be reserved.
@@ -262,7 +318,8 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             f.C = last ? (float *)C : buf[i & 1];
             f.ldc = last ? ldc : ldN;
             f.kblock = 0;  // the multigemm FP32 chain does not split K (kernel_f32.h:3)
-            int st = launch(launch_ffma_sgemm(f, c->sms, c->stream), "ffma stage");
+            int st = run_kernel(c, FG_PK_FFMA, gemm_flops(M[i], N, K[i]), "ffma stage",
+                                [&] { return launch_ffma_sgemm(f, c->sms, c->stream); });
             if (st) return st;
             x = f.C;
             ldx = f.ldc;
@@ -281,15 +338,17 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             const long ldk = round_up(K[i], 4);
             wh[i] = (float *)arena_take(c, (size_t)M[i] * ldk * 4);
             wl[i] = (float *)arena_take(c, (size_t)M[i] * ldk * 4);
-            int st = launch(launch_split_tf32((const float *)a[i].p, a[i].ld, wh[i], wl[i], ldk,
-                                              M[i], K[i], c->stream),
-                            "tf32 split (weights)");
+            int st = run_kernel(c, FG_PK_AUX, 0.0, "tf32 split (weights)", [&] {
+                return launch_split_tf32((const float *)a[i].p, a[i].ld, wh[i], wl[i], ldk, M[i],
+                                         K[i], c->stream);
+            });
             if (st) return st;
         }
         float *xh = (float *)arena_take(c, (size_t)K[0] * ldN * 4);
         float *xl = (float *)arena_take(c, (size_t)K[0] * ldN * 4);
-        int st = launch(launch_split_tf32((const float *)b.p, b.ld, xh, xl, ldN, K[0], N, c->stream),
-                        "tf32 split (activations)");
+        int st = run_kernel(c, FG_PK_AUX, 0.0, "tf32 split (activations)", [&] {
+            return launch_split_tf32((const float *)b.p, b.ld, xh, xl, ldN, K[0], N, c->stream);
+        });
         if (st) return st;
         float *ph[2] = {nullptr, nullptr}, *pl[2] = {nullptr, nullptr};
         if (n > 1)
@@ -309,7 +368,9 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             s.ld_out = last ? ldc : ldN;
             s.m_written = (int)M[i];
             s.tail_lo = s.tail_hi = 0;
-            st = launch(launch_tc_stage(s, c->sms, c->stream), "tf32x3 stage");
+            s.kchunk = tf32_chunk_blocks(K[i]);
+            st = run_kernel(c, FG_PK_TC_TF32X3, gemm_flops(M[i], N, K[i]), "tf32x3 stage",
+                            [&] { return launch_tc_stage(s, c->sms, c->stream); });
             if (st) return st;
             xh = ph[i & 1];
             xl = pl[i & 1];
@@ -348,7 +409,8 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             s.permute = ref ? 1 : 0;
             s.m_written = (int)M[i];
             s.tail_lo = s.tail_hi = 0;
-            int st = launch(launch_tc_stage(s, c->sms, c->stream), "bf16 stage");
+            int st = run_kernel(c, FG_PK_TC_BF16, gemm_flops(M[i], N, K[i]), "bf16 stage",
+                                [&] { return launch_tc_stage(s, c->sms, c->stream); });
             if (st) return st;
             x = s.out;
             ldx = s.ld_out;
@@ -376,9 +438,10 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             }
             const long ldw = round_up(Ki + 4, 16);
             uint8_t *wp = (uint8_t *)arena_take(c, (size_t)Mi * ldw);
-            int st = launch(launch_prep_int8_weights((const int8_t *)a[i].p, a[i].ld, wp, ldw, Mi,
-                                                     Ki, tail_lo, tail_hi, c->stream),
-                            "int8 weight prep");
+            int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 weight prep", [&] {
+                return launch_prep_int8_weights((const int8_t *)a[i].p, a[i].ld, wp, ldw, Mi, Ki,
+                                                tail_lo, tail_hi, c->stream);
+            });
             if (st) return st;
             const bool last = (i == n - 1);
             s.op = OP_I8;
@@ -392,7 +455,8 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             s.m_written = (last && ref) ? (int)((Mi / 4) * 4) : (int)Mi;
             s.tail_lo = (int)tail_lo;
             s.tail_hi = (int)tail_hi;
-            st = launch(launch_tc_stage(s, c->sms, c->stream), "int8 stage");
+            st = run_kernel(c, FG_PK_TC_I8, gemm_flops(Mi, N, Ki), "int8 stage",
+                            [&] { return launch_tc_stage(s, c->sms, c->stream); });
             if (st) return st;
             x = s.out;
             ldx = s.ld_out;
@@ -495,7 +559,8 @@ int run_sgemm(DevCtx *c, int algo, float *C, long ldc, const float *A, long lda,
         f.M = (int)M; f.N = (int)N; f.K = (int)K;
         f.A = A; f.lda = lda; f.B = B; f.ldb = ldb; f.C = C; f.ldc = ldc;
         f.kblock = kblock;
-        return launch(launch_ffma_sgemm(f, c->sms, c->stream), "ffma sgemm");
+        return run_kernel(c, FG_PK_FFMA, gemm_flops(M, N, K), "ffma sgemm",
+                          [&] { return launch_ffma_sgemm(f, c->sms, c->stream); });
     }
     Mat a{A, lda};
     return run_chain(c, FG_DT_F32, FG_SEM_MATH, FG_F32_3XTF32, C, ldc, Mat{B, ldb}, N, 1, &a, &M, &K);
@@ -732,5 +797,48 @@ FG_EXPORT int fg_sync(void)
     std::lock_guard<std::mutex> lk(c->mu);
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     if ((st = collect_status(c))) return st;
+    return ok();
+}
+
+FG_EXPORT int fg_profile_begin(void)
+{
+    DevCtx *c;
+    int st;
+    if ((st = get_ctx(&c))) return st;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (auto &r : c->prof) c->prof_pool.push_back(r);
+    c->prof.clear();
+    g_prof_on.store(1);
+    return ok();
+}
+
+FG_EXPORT int fg_profile_end(void)
+{
+    g_prof_on.store(0);
+    return ok();
+}
+
+FG_EXPORT int fg_profile_query(int kind, double *total_ms, unsigned long long *launches,
+                               double *flops)
+{
+    DevCtx *c;
+    int st;
+    if ((st = get_ctx(&c))) return st;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    double ms = 0.0, fl = 0.0;
+    unsigned long long n = 0;
+    for (auto &r : c->prof) {
+        if (kind >= 0 && r.kind != kind) continue;
+        float t = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&t, r.a, r.b));
+        ms += t;
+        fl += r.flops;
+        ++n;
+    }
+    if (total_ms) *total_ms = ms;
+    if (launches) *launches = n;
+    if (flops) *flops = fl;
     return ok();
 }

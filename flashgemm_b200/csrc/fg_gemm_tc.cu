@@ -85,7 +85,10 @@ struct Geometry {
     static constexpr int B_KSTEP_BYTES = (MMA_K_BYTES / T::elt) * kRowBytes;
     // stride between k-row groups of the B swizzle atom: 8 rows (16B chunks) or 4 rows (32B)
     static constexpr int B_SBO = T::b_layout == SMEM_SW128_32B ? 512 : 1024;
-    static constexpr int TMEM_COLS = 2 * T::BN;
+    // 3xTF32 keeps the small hi*lo + lo*hi terms in their own accumulator next to
+    // hi*hi: each of the two TMEM buffers is then [hi*hi | corrections].
+    static constexpr int ACC_COLS = (T::split ? 2 : 1) * T::BN;
+    static constexpr int TMEM_COLS = 2 * ACC_COLS;
     static constexpr int SMEM_BYTES = T::STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*bars*/;
 };
 
@@ -133,7 +136,11 @@ __device__ __forceinline__ void store_chunk(const StageArgs &p, int row, int n0,
 {
     const int N = p.N;
     const bool full = (n0 + 32 <= N);
-    switch (p.epi) {
+    // each operand kind reaches only its own epilogues; keep the others out of its code
+    const int epi = OP == OP_BF16 ? (p.epi == EPI_BF16 ? EPI_BF16 : EPI_F32)
+                  : OP == OP_I8   ? (p.epi == EPI_S8 ? EPI_S8 : EPI_S32)
+                                  : (p.epi == EPI_TF32SPLIT ? EPI_TF32SPLIT : EPI_F32);
+    switch (epi) {
     case EPI_F32:
     case EPI_S32: {
         if (row >= p.m_written) return;
@@ -271,6 +278,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int tiles_n = (p.N + BN - 1) / BN;
     const int num_tiles = tiles_m * tiles_n;
     const int num_kb = (p.K + G::BK - 1) / G::BK;
+    // k-blocks per accumulator hand-off. 3xTF32 hands partial sums to the
+    // epilogue every p.kchunk blocks, which adds them in FP32 registers with
+    // round-to-nearest: the tensor core's own FP32 accumulation over long K
+    // drifts well above an FFMA loop's rounding error, short chunks do not.
+    const int kchunk = (T::split && p.kchunk > 0) ? p.kchunk : num_kb;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
@@ -356,60 +368,63 @@ __global__ void __launch_bounds__(kThreads, 1)
             int acc = 0;
             uint32_t acc_ph = 0;
             for (int t = blockIdx.x; t < num_tiles; t += gridDim.x) {
-                if (!mbar_wait(&bars->acc_empty[acc], acc_ph ^ 1, p.status, KERR_WAIT_ACC_EMPTY)) {
-                    set_abort(bars);
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t d_tmem = tmem_base + acc * BN;
-                bool ok = true;
-                for (int kb = 0; kb < num_kb; ++kb) {
-                    if (!mbar_wait(&bars->full[s], ph, p.status, KERR_WAIT_FULL)) {
-                        ok = false;
-                        break;
+                // one accumulator hand-off per chunk of k-blocks (the whole K unless
+                // the epilogue promotes partial sums, see kchunk)
+                for (int kc = 0; kc < num_kb; kc += kchunk) {
+                    if (!mbar_wait(&bars->acc_empty[acc], acc_ph ^ 1, p.status,
+                                   KERR_WAIT_ACC_EMPTY)) {
+                        set_abort(bars);
+                        goto mma_done;
                     }
                     tc_fence_after();
-                    const uint32_t a_addr = smem_u32(smem + s * G::STAGE_BYTES);
-                    const uint32_t b_addr = a_addr + G::A_BYTES;
+                    const uint32_t d_tmem = tmem_base + acc * G::ACC_COLS;
+                    const int kend = kc + kchunk < num_kb ? kc + kchunk : num_kb;
+                    for (int kb = kc; kb < kend; ++kb) {
+                        if (!mbar_wait(&bars->full[s], ph, p.status, KERR_WAIT_FULL)) {
+                            set_abort(bars);
+                            goto mma_done;
+                        }
+                        tc_fence_after();
+                        const uint32_t a_addr = smem_u32(smem + s * G::STAGE_BYTES);
+                        const uint32_t b_addr = a_addr + G::A_BYTES;
 #pragma unroll
-                    for (int k = 0; k < G::MMAS_PER_STAGE; ++k) {
-                        const uint64_t ad =
-                            smem_desc(a_addr + k * G::MMA_K_BYTES, 16, 1024, SMEM_SW128);
-                        const uint64_t bd = smem_desc(b_addr + k * G::B_KSTEP_BYTES, G::BOX_BYTES,
-                                                      G::B_SBO, T::b_layout);
-                        const uint32_t accumulate = (kb | k) != 0;
-                        if constexpr (T::split) {
-                            const uint32_t lo_off = G::A_BYTES + G::B_BYTES;
-                            const uint64_t ad_lo = smem_desc(a_addr + lo_off + k * G::MMA_K_BYTES,
-                                                             16, 1024, SMEM_SW128);
-                            const uint64_t bd_lo =
-                                smem_desc(b_addr + lo_off + k * G::B_KSTEP_BYTES, G::BOX_BYTES,
-                                          G::B_SBO, T::b_layout);
-                            // small terms first: hi*lo + lo*hi + hi*hi
-                            tc_mma<T::kind>(d_tmem, ad, bd_lo, T::idesc, accumulate);
-                            tc_mma<T::kind>(d_tmem, ad_lo, bd, T::idesc, 1);
-                            tc_mma<T::kind>(d_tmem, ad, bd, T::idesc, 1);
-                        } else {
-                            tc_mma<T::kind>(d_tmem, ad, bd, T::idesc, accumulate);
+                        for (int k = 0; k < G::MMAS_PER_STAGE; ++k) {
+                            const uint64_t ad =
+                                smem_desc(a_addr + k * G::MMA_K_BYTES, 16, 1024, SMEM_SW128);
+                            const uint64_t bd = smem_desc(b_addr + k * G::B_KSTEP_BYTES,
+                                                          G::BOX_BYTES, G::B_SBO, T::b_layout);
+                            const uint32_t accumulate = (kb != kc || k != 0);
+                            if constexpr (T::split) {
+                                const uint32_t lo_off = G::A_BYTES + G::B_BYTES;
+                                const uint64_t ad_lo = smem_desc(
+                                    a_addr + lo_off + k * G::MMA_K_BYTES, 16, 1024, SMEM_SW128);
+                                const uint64_t bd_lo =
+                                    smem_desc(b_addr + lo_off + k * G::B_KSTEP_BYTES,
+                                              G::BOX_BYTES, G::B_SBO, T::b_layout);
+                                // hi*lo + lo*hi into the correction accumulator, whose
+                                // rounding is 2^-11 smaller; hi*hi alone into the main one
+                                tc_mma<T::kind>(d_tmem + BN, ad, bd_lo, T::idesc, accumulate);
+                                tc_mma<T::kind>(d_tmem + BN, ad_lo, bd, T::idesc, 1);
+                                tc_mma<T::kind>(d_tmem, ad, bd, T::idesc, accumulate);
+                            } else {
+                                tc_mma<T::kind>(d_tmem, ad, bd, T::idesc, accumulate);
+                            }
+                        }
+                        tc_commit(&bars->empty[s]);  // stage free once these MMAs retire
+                        if (++s == S) {
+                            s = 0;
+                            ph ^= 1;
                         }
                     }
-                    tc_commit(&bars->empty[s]);  // stage free once these MMAs retire
-                    if (++s == S) {
-                        s = 0;
-                        ph ^= 1;
+                    tc_commit(&bars->acc_full[acc]);  // accumulator ready once its MMAs retire
+                    if (++acc == 2) {
+                        acc = 0;
+                        acc_ph ^= 1;
                     }
-                }
-                if (!ok) {
-                    set_abort(bars);
-                    break;
-                }
-                tc_commit(&bars->acc_full[acc]);  // accumulator ready once all MMAs retire
-                if (++acc == 2) {
-                    acc = 0;
-                    acc_ph ^= 1;
                 }
                 if (aborted(bars)) break;
             }
+        mma_done:
             // all MMAs this thread issued have retired before TMEM is released
             tc_commit(&bars->mma_done);
             mbar_wait(&bars->mma_done, 0, p.status, KERR_WAIT_FULL);
@@ -419,6 +434,63 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int quarter = warp & 3;  // TMEM lane quarter this warp may access
         int acc = 0;
         uint32_t acc_ph = 0;
+        if constexpr (T::split) {
+            for (int t = blockIdx.x; t < num_tiles; t += gridDim.x) {
+                const int m0 = (t / tiles_n) * kBM;
+                const int n0 = (t % tiles_n) * BN;
+                const int row = m0 + quarter * 32 + lane;
+                float sum[BN / 32][32];
+#pragma unroll
+                for (int c = 0; c < BN / 32; ++c)
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) sum[c][j] = 0.f;
+                bool ok = true;
+                for (int kc = 0; kc < num_kb; kc += kchunk) {
+                    if (!mbar_wait(&bars->acc_full[acc], acc_ph, p.status, KERR_WAIT_ACC_FULL)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t t_row =
+                        tmem_base + acc * G::ACC_COLS + ((uint32_t)(quarter * 32) << 16);
+#pragma unroll
+                    for (int c = 0; c < BN / 32; ++c) {
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            uint32_t v[16], w[16];
+                            tmem_ld_32x32b_x16(t_row + c * 32 + 16 * h, v);
+                            tmem_ld_32x32b_x16(t_row + BN + c * 32 + 16 * h, w);
+                            tmem_ld_wait();
+#pragma unroll
+                            for (int j = 0; j < 16; ++j)
+                                sum[c][16 * h + j] = sum[c][16 * h + j] +
+                                                     (__uint_as_float(v[j]) + __uint_as_float(w[j]));
+                        }
+                    }
+                    tc_fence_before();
+                    mbar_arrive(&bars->acc_empty[acc]);
+                    if (++acc == 2) {
+                        acc = 0;
+                        acc_ph ^= 1;
+                    }
+                }
+                if (!ok) {
+                    set_abort(bars);
+                    break;
+                }
+#pragma unroll
+                for (int c = 0; c < BN / 32; ++c) {
+                    const int nc = n0 + c * 32;
+                    if (nc < p.N && row < p.M) {
+                        uint32_t v[32];
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) v[j] = __float_as_uint(sum[c][j]);
+                        store_chunk<OP>(p, row, nc, v);
+                    }
+                }
+                if (aborted(bars)) break;
+            }
+        } else
         for (int t = blockIdx.x; t < num_tiles; t += gridDim.x) {
             if (!mbar_wait(&bars->acc_full[acc], acc_ph, p.status, KERR_WAIT_ACC_FULL)) {
                 set_abort(bars);
@@ -428,7 +500,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int m0 = (t / tiles_n) * kBM;
             const int n0 = (t % tiles_n) * BN;
             const int row = m0 + quarter * 32 + lane;
-            const uint32_t t_row = tmem_base + acc * BN + ((uint32_t)(quarter * 32) << 16);
+            const uint32_t t_row = tmem_base + acc * G::ACC_COLS + ((uint32_t)(quarter * 32) << 16);
             const bool tail = (row >= p.tail_lo && row < p.tail_hi);
             uint32_t wq = 0;
             if (tail) wq = *reinterpret_cast<const uint32_t *>(

@@ -37,6 +37,7 @@ struct StageArgs {
     int m_written;     // rows >= m_written are not stored (INT8 reference semantics)
     int tail_lo;       // INT8 reference tail rows [tail_lo, tail_hi): weights pre-shifted,
     int tail_hi;       //   first k-quad kept at w[m * ld_w + K .. +3], added in the epilogue
+    int kchunk;        // TF32X3: k-blocks (of 32) per FP32 promotion of the partial sum
     int *status;       // device status word (0 = ok)
 };
 

@@ -87,6 +87,22 @@ int fg_sync(void);
  * Lets a benchmark count its own launches. */
 unsigned long long fg_kernel_launches(void);
 
+/* Per-launch device timing. While profiling is on, every kernel the library
+ * launches on the current device is bracketed by CUDA events on the stream it
+ * runs on. fg_profile_query sums, for one kernel class (or -1 for all), the
+ * device time in ms, the number of launches and the algorithmic FLOPs
+ * (2*M*N*K per GEMM stage). */
+enum {
+    FG_PK_TC_BF16 = 0,   /* tensor-core stage, BF16 */
+    FG_PK_TC_I8 = 1,     /* tensor-core stage, INT8 */
+    FG_PK_TC_TF32X3 = 2, /* tensor-core stage, 3xTF32 */
+    FG_PK_FFMA = 3,      /* CUDA-core FP32 GEMM */
+    FG_PK_AUX = 4        /* splits, weight preparation */
+};
+int fg_profile_begin(void);
+int fg_profile_end(void);
+int fg_profile_query(int kind, double *total_ms, unsigned long long *launches, double *flops);
+
 /* Library version string. */
 const char *fg_version(void);
 
