@@ -624,6 +624,12 @@ bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
 
 }  // namespace
 
+// Status setters for the library's other host files (fg_noalloc.cu).
+namespace fg {
+int api_fail(int status, const char *msg) { return fail(status, "%s", msg); }
+int api_ok() { return ok(); }
+}  // namespace fg
+
 // ==================================================================== C ABI
 
 FG_EXPORT int flashgemm_thread_num = 1;

@@ -103,6 +103,41 @@ int fg_profile_begin(void);
 int fg_profile_end(void);
 int fg_profile_query(int kind, double *total_ms, unsigned long long *launches, double *flops);
 
+/* Size of the fixed device array fg_chain_bf16_noalloc keeps its
+ * between-stage buffers in: 48 MiB, present on every GPU that loads the library
+ * until the process exits. */
+#define FG_NOALLOC_SCRATCH_BYTES (48u << 20)
+
+/* BF16 chain that allocates no device memory. No counterpart in the reference
+ * (whose chain allocates and frees host scratch on every call).
+ *
+ * For callers that cannot call cudaMalloc when they run a chain: a framework
+ * whose device memory all belongs to its own pool, a serving process that must
+ * not grow its footprint after start-up. Same operands and semantics as
+ * fg_chain_dev(FG_DT_BF16, ...) (device pointers: B K[0] x N, A[i] M[i] x K[i],
+ * C M[n-1] x N float, dense rows), but the between-stage activations live in a
+ * fixed array of FG_NOALLOC_SCRATCH_BYTES inside the library, and the kernels
+ * run directly on `stream` (NULL: the legacy default stream). Nothing is
+ * allocated or freed: no cudaMalloc, no cudaFree, no allocating library call.
+ *
+ * Limits: the largest two intermediates of alternating stages, each
+ * M_i x round_up(N, 16) BF16 values, must fit in the array together
+ * (FG_ERR_INVALID with the sizes otherwise; e.g. N = 4096 with widths
+ * 4096 and 1024 needs 40 MiB); N and every K must be multiples of 8 and all
+ * pointers 16-byte aligned.
+ *
+ * The array is shared by every call on a device and keeps the last call's
+ * contents: calls whose kernels overlap on the GPU race, so order them (one
+ * stream, or events). `status`, if not NULL, is a device int the kernels set
+ * to a nonzero code when a bounded pipeline wait runs out (the caller clears
+ * it); with NULL the kernels use a word of the array that every call clears.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and the SM count; make that first call before any
+ * stream capture. Returns a fg_status; the message is in fg_last_error(). */
+int fg_chain_bf16_noalloc(float *C, const uint16_t *B, long N, int num_gemm,
+                          const uint16_t *const *A, const long *M, const long *K, int *status,
+                          void *stream);
+
 /* Library version string. */
 const char *fg_version(void);
 
