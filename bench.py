@@ -39,11 +39,15 @@ WORKLOADS = {
     "bf16-chain": ("bf16", 4096, 1024, [4096, 1024, 1024]),
     "int8-chain": ("int8", 8192, 2048, [4096, 2048, 4096, 1024]),
     "f32-gemm": ("f32", 1024, 1024, [1024]),
+    "bf16-gemm": ("bf16", 8192, 8192, [8192]),
+    "int8-gemm": ("int8", 8192, 8192, [8192]),
 }
 DESCR = {
     "bf16-chain": "BF16 chain of 3 GEMMs: X[4096x1024]*W1[1024x4096]*W2[4096x1024]*W3[1024x1024]",
     "int8-chain": "INT8 chain of 4 GEMMs: X[8192x2048]*W1..W4, widths 2048->4096->2048->4096->1024",
     "f32-gemm": "single FP32 GEMM C=A*B, M=N=K=1024 (plain FP32 FMA kernel)",
+    "bf16-gemm": "single BF16 GEMM (one-stage chain) M=N=K=8192, the shape of the cuBLAS peak",
+    "int8-gemm": "single INT8 GEMM (one-stage chain) M=N=K=8192",
 }
 
 

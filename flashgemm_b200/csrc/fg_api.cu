@@ -99,6 +99,7 @@ int sgemm_algo()
 }
 
 inline long round_up(long x, long a) { return (x + a - 1) / a * a; }
+inline bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
 
 // 3xTF32: k-blocks of 32 between FP32 promotions of the tensor-core partial sum.
 // The tensor core's FP32 accumulation error grows with the number of MMAs that
@@ -237,8 +238,19 @@ size_t chain_scratch(int dtype, int algo, long N, int n, const long *M, const lo
     size_t s = 0;
     long maxM = 0;
     for (int i = 0; i < n - 1; ++i) maxM = M[i] > maxM ? M[i] : maxM;
+    if (dtype == FG_DT_INT8 || dtype == FG_DT_BF16) {  // fused-chain completion counters
+        s += carve_size((size_t)n * ((N + 255) / 256) * sizeof(int));
+        if (getenv("FG_TRACE_DIR")) {  // per-tile timeline of the fused kernel
+            size_t items = 0;
+            for (int i = 0; i < n; ++i) items += (size_t)((M[i] + 255) / 256) * ((N + 255) / 256);
+            s += carve_size(items * 2 * 9 * 8);
+        }
+    }
     if (dtype == FG_DT_INT8) {
-        for (int i = 0; i < n; ++i) s += carve_size((size_t)M[i] * round_up(K[i] + 4, 16));
+        for (int i = 0; i < n; ++i) {  // padded copy (unaligned rows) + tail block (<= 267 rows)
+            s += carve_size((size_t)M[i] * round_up(K[i] + 4, 16));
+            s += carve_size((size_t)(M[i] < 272 ? M[i] : 272) * round_up(K[i] + 4, 16));
+        }
         s += 2 * carve_size((size_t)maxM * ldN);
     } else if (dtype == FG_DT_BF16) {
         for (int i = 0; i < n; ++i)
@@ -287,8 +299,86 @@ int run_kernel(DevCtx *c, int kind, double flops, const char *what, Fn &&fn)
     return st;
 }
 
-int tc_kind(int op) { return op == OP_BF16 ? FG_PK_TC_BF16 : op == OP_I8 ? FG_PK_TC_I8 : FG_PK_TC_TF32X3; }
 double gemm_flops(long M, long N, long K) { return 2.0 * (double)M * (double)N * (double)K; }
+
+// Whole chain in one fused launch when possible (FG_FUSED=0 turns it off),
+// else one tensor-core launch per stage: the per-GEMM path.
+bool fused_enabled()
+{
+    static const bool on = [] {
+        const char *v = getenv("FG_FUSED");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+bool g_fused_unsupported[64];
+
+int launch_stages(DevCtx *c, int kind, std::vector<StageArgs> &stages, long N)
+{
+    const int n = (int)stages.size();
+    if (fused_enabled() && n <= chain_max_stages() && !g_fused_unsupported[c->dev & 63]) {
+        const long tiles_n = (N + 255) / 256;
+        int *done = (int *)arena_take(c, (size_t)n * tiles_n * sizeof(int));
+        CUDA_TRY(cudaMemsetAsync(done, 0, (size_t)n * tiles_n * sizeof(int), c->stream));
+        double fl = 0.0;
+        for (auto &st : stages) fl += gemm_flops(st.M, st.N, st.K);
+        // FG_TRACE_DIR=<dir>: write a per-tile timeline of every fused launch there
+        // (synchronises after the launch: a diagnostic, not for timing runs)
+        static const char *trace_dir = getenv("FG_TRACE_DIR");
+        unsigned long long *trace = nullptr;
+        size_t trace_words = 0;
+        if (trace_dir) {
+            size_t items = 0;
+            for (auto &sa : stages) items += (size_t)((sa.M + 255) / 256) * tiles_n;
+            trace_words = items * 2 * chain_trace_fields();
+            trace = (unsigned long long *)arena_take(c, trace_words * 8);
+            CUDA_TRY(cudaMemsetAsync(trace, 0, trace_words * 8, c->stream));
+        }
+        cudaError_t le = cudaSuccess;
+        int st = run_kernel(c, kind, fl, "fused chain", [&] {
+            le = launch_tc_chain(stages.data(), n, done, c->status, trace, c->sms, c->stream);
+            return le;
+        });
+        if (st == FG_OK && trace) {
+            std::vector<unsigned long long> h(trace_words);
+            CUDA_TRY(cudaMemcpyAsync(h.data(), trace, trace_words * 8, cudaMemcpyDeviceToHost,
+                                     c->stream));
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            static int seq = 0;
+            char path[1024];
+            snprintf(path, sizeof path, "%s/chain_trace_%d.csv", trace_dir, seq++);
+            if (FILE *f = fopen(path, "w")) {
+                fprintf(f, "item,cta,sm,prod_start,dep_done,prod_end,mma_start,mma_end,epi_start,"
+                           "epi_end\n");
+                const int nf = chain_trace_fields();
+                for (size_t r = 0; r < trace_words / nf; ++r) {
+                    fprintf(f, "%zu,%zu", r / 2, r % 2);
+                    for (int k = 0; k < nf; ++k) fprintf(f, ",%llu", h[r * nf + k]);
+                    fprintf(f, "\n");
+                }
+                fclose(f);
+            }
+        }
+        if (st == FG_OK) return FG_OK;
+        if (le != cudaErrorNotSupported && le != cudaErrorCooperativeLaunchTooLarge &&
+            le != cudaErrorInvalidConfiguration)
+            return st;
+        // this device cannot co-schedule the fused grid: per-stage launches from now on
+        cudaGetLastError();
+        fprintf(stderr, "flashgemm-b200: fused chain launch unavailable on device %d (%s); "
+                        "running one launch per stage\n", c->dev, cudaGetErrorString(le));
+        g_launches.fetch_sub(1, std::memory_order_relaxed);
+        g_fused_unsupported[c->dev & 63] = true;
+        ok();
+    }
+    for (auto &s : stages) {
+        int st = run_kernel(c, kind, gemm_flops(s.M, s.N, s.K),
+                            kind == FG_PK_TC_BF16 ? "bf16 stage" : "int8 stage",
+                            [&] { return launch_tc_stage(s, c->sms, c->stream); });
+        if (st) return st;
+    }
+    return FG_OK;
+}
 
 // Runs the chain on c->stream. Device operands: B (K[0] x N, ld b.ld),
 // A[i] (M[i] x K[i], ld a[i].ld, 16-byte-aligned rows where the tensor path
@@ -386,6 +476,7 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
         }
         const void *x = b.p;
         long ldx = b.ld;
+        std::vector<StageArgs> stages;
         for (int i = 0; i < n; ++i) {
             const void *w = a[i].p;
             long ldw = a[i].ld;
@@ -409,13 +500,11 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             s.permute = ref ? 1 : 0;
             s.m_written = (int)M[i];
             s.tail_lo = s.tail_hi = 0;
-            int st = run_kernel(c, FG_PK_TC_BF16, gemm_flops(M[i], N, K[i]), "bf16 stage",
-                                [&] { return launch_tc_stage(s, c->sms, c->stream); });
-            if (st) return st;
+            stages.push_back(s);
             x = s.out;
             ldx = s.ld_out;
         }
-        return FG_OK;
+        return launch_stages(c, FG_PK_TC_BF16, stages, N);
     }
 
     // INT8
@@ -427,6 +516,7 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
         }
         const void *x = b.p;
         long ldx = b.ld;
+        std::vector<StageArgs> stages;
         for (int i = 0; i < n; ++i) {
             const long Mi = M[i], Ki = K[i];
             // reference tail rows (multigemm/src/kernel_int8.h:771-1057): only with
@@ -436,17 +526,42 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
                 tail_lo = (Mi / 12) * 12;
                 tail_hi = (Mi / 4) * 4;
             }
+            // Weights go to the MMA as they are when their rows are 16-byte aligned
+            // (TMA); otherwise through a padded copy. Tail rows always come from a
+            // prepared copy of the 256-row block that holds them.
             const long ldw = round_up(Ki + 4, 16);
-            uint8_t *wp = (uint8_t *)arena_take(c, (size_t)Mi * ldw);
-            int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 weight prep", [&] {
-                return launch_prep_int8_weights((const int8_t *)a[i].p, a[i].ld, wp, ldw, Mi, Ki,
-                                                tail_lo, tail_hi, c->stream);
-            });
-            if (st) return st;
+            const void *wmain = a[i].p;
+            long ldmain = a[i].ld;
+            if ((ldmain % 16) || !aligned16(wmain)) {
+                uint8_t *wp = (uint8_t *)arena_take(c, (size_t)Mi * ldw);
+                int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 weight copy", [&] {
+                    return launch_prep_int8_weights((const int8_t *)a[i].p, a[i].ld, wp, ldw, Mi,
+                                                    Ki, 0, 0, c->stream);
+                });
+                if (st) return st;
+                wmain = wp;
+                ldmain = ldw;
+            }
+            s.w_tail = nullptr;
+            s.ld_w_tail = 0;
+            s.tail_row0 = 0;
+            if (tail_hi > tail_lo) {
+                const long row0 = (tail_lo / 256) * 256;
+                uint8_t *wt = (uint8_t *)arena_take(c, (size_t)(Mi - row0) * ldw);
+                int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 tail-row prep", [&] {
+                    return launch_prep_int8_weights((const int8_t *)a[i].p + row0 * a[i].ld,
+                                                    a[i].ld, wt, ldw, Mi - row0, Ki,
+                                                    tail_lo - row0, tail_hi - row0, c->stream);
+                });
+                if (st) return st;
+                s.w_tail = wt;
+                s.ld_w_tail = ldw;
+                s.tail_row0 = (int)row0;
+            }
             const bool last = (i == n - 1);
             s.op = OP_I8;
             s.M = (int)Mi; s.K = (int)Ki;
-            s.w = wp; s.ld_w = ldw;
+            s.w = wmain; s.ld_w = ldmain;
             s.x = x; s.ld_x = ldx;
             s.epi = last ? EPI_S32 : EPI_S8;
             s.out = last ? C : (void *)buf[i & 1];
@@ -455,13 +570,11 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             s.m_written = (last && ref) ? (int)((Mi / 4) * 4) : (int)Mi;
             s.tail_lo = (int)tail_lo;
             s.tail_hi = (int)tail_hi;
-            st = run_kernel(c, FG_PK_TC_I8, gemm_flops(Mi, N, Ki), "int8 stage",
-                            [&] { return launch_tc_stage(s, c->sms, c->stream); });
-            if (st) return st;
+            stages.push_back(s);
             x = s.out;
             ldx = s.ld_out;
         }
-        return FG_OK;
+        return launch_stages(c, FG_PK_TC_I8, stages, N);
     }
 }
 
@@ -619,8 +732,6 @@ int fence_out(DevCtx *c, void *user)
     CUDA_TRY(cudaStreamWaitEvent((cudaStream_t)user, c->ev_out, 0));
     return FG_OK;
 }
-
-bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
 
 }  // namespace
 

@@ -47,25 +47,39 @@ cudaError_t launch_split_tf32(const float *in, long ld_in, float *hi, float *lo,
 // so a plain MMA yields sum_{s>=1} A_q(s) X_q(s-1); the missing A_q(0) X_q(0)
 // term is added by the GEMM epilogue from the first quad kept at [K, K + 4).
 // Other rows are copied unchanged; columns [K, ld_out) of them are zero.
+// One thread writes 16 bytes (ld_out is a multiple of 16).
 __global__ void prep_int8_weights_kernel(const int8_t *__restrict__ src, long ld_in,
                                          uint8_t *__restrict__ dst, long ld_out, long M, long K,
                                          long tail_lo, long tail_hi)
 {
-    const long total = M * ld_out;
+    const long per_row = ld_out / 16;
+    const long total = M * per_row;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
          i += (long)gridDim.x * blockDim.x) {
-        const long m = i / ld_out, k = i - m * ld_out;
+        const long m = i / per_row, k0 = (i - m * per_row) * 16;
         const uint8_t *row = reinterpret_cast<const uint8_t *>(src) + m * ld_in;
-        uint8_t v = 0;
-        if (m >= tail_lo && m < tail_hi) {
-            if (k < K - 4)
-                v = row[k + 4];
-            else if (k >= K && k < K + 4)
-                v = row[k - K];
-        } else if (k < K) {
-            v = row[k];
+        const bool tail = (m >= tail_lo && m < tail_hi);
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint32_t word = 0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const long k = k0 + 4 * q + b;
+                uint8_t v = 0;
+                if (tail) {
+                    if (k < K - 4)
+                        v = row[k + 4];
+                    else if (k >= K && k < K + 4)
+                        v = row[k - K];
+                } else if (k < K) {
+                    v = row[k];
+                }
+                word |= (uint32_t)v << (8 * b);
+            }
+            w[q] = word;
         }
-        dst[i] = v;
+        *reinterpret_cast<uint4 *>(dst + m * ld_out + k0) = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
 
@@ -73,7 +87,8 @@ cudaError_t launch_prep_int8_weights(const int8_t *src, long ld_in, uint8_t *dst
                                      long M, long K, long tail_lo, long tail_hi, cudaStream_t s)
 {
     if (M <= 0) return cudaSuccess;
-    const long total = M * ld_out;
+    if (ld_out % 16) return cudaErrorInvalidValue;
+    const long total = M * (ld_out / 16);
     long blocks = (total + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
     prep_int8_weights_kernel<<<(unsigned)blocks, 256, 0, s>>>(src, ld_in, dst, ld_out, M, K,

@@ -21,238 +21,11 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
-#include <mutex>
+#include <cstdlib>
 
-#include "fg_kernels.h"
-#include "fg_ptx.cuh"
+#include "fg_tc_common.cuh"
 
 namespace fg {
-
-constexpr int kBM = 128;          // MMA M (weight rows per tile)
-constexpr int kRowBytes = 128;    // K extent of a stage in bytes (one 128B swizzle row)
-constexpr int kThreads = 192;
-
-template <int OP>
-struct OpTraits;
-template <>
-struct OpTraits<OP_BF16> {
-    static constexpr MmaKind kind = MmaKind::F16;
-    static constexpr int elt = 2;
-    static constexpr int BN = 256;
-    static constexpr int STAGES = 4;
-    static constexpr bool split = false;
-    static constexpr uint32_t b_layout = SMEM_SW128;
-    // D F32, A BF16, B BF16, A K-major, B MN-major
-    static constexpr uint32_t idesc = make_idesc(1, 1, 1, 0, 1, kBM, BN);
-};
-template <>
-struct OpTraits<OP_I8> {
-    static constexpr MmaKind kind = MmaKind::I8;
-    static constexpr int elt = 1;
-    static constexpr int BN = 256;
-    static constexpr int STAGES = 4;
-    static constexpr bool split = false;
-    static constexpr uint32_t b_layout = SMEM_SW128;
-    // D S32, A U8 (the reference reads weights unsigned), B S8, A K-major, B MN-major
-    static constexpr uint32_t idesc = make_idesc(2, 0, 1, 0, 1, kBM, BN);
-};
-template <>
-struct OpTraits<OP_TF32X3> {
-    static constexpr MmaKind kind = MmaKind::TF32;
-    static constexpr int elt = 4;
-    static constexpr int BN = 128;
-    static constexpr int STAGES = 3;
-    static constexpr bool split = true;
-    // MN-major TF32 needs the 32-byte-chunk 128B swizzle (atoms of 4 k-rows)
-    static constexpr uint32_t b_layout = SMEM_SW128_32B;
-    // D F32, A TF32, B TF32, A K-major, B MN-major
-    static constexpr uint32_t idesc = make_idesc(1, 2, 2, 0, 1, kBM, BN);
-};
-
-template <int OP>
-struct Geometry {
-    using T = OpTraits<OP>;
-    static constexpr int BK = kRowBytes / T::elt;              // K elements per stage
-    static constexpr int A_BYTES = kBM * kRowBytes;            // 16 KB
-    static constexpr int BOX_N = kRowBytes / T::elt;           // MN-major box width (elements)
-    static constexpr int BOX_BYTES = BOX_N * BK * T::elt;      // one B box
-    static constexpr int NBOX = T::BN / BOX_N;
-    static constexpr int B_BYTES = NBOX * BOX_BYTES;           // BN x BK elements
-    static constexpr int PARTS = T::split ? 2 : 1;             // hi / lo
-    static constexpr int STAGE_BYTES = PARTS * (A_BYTES + B_BYTES);
-    static constexpr int MMA_K_BYTES = 32;                     // K per MMA, A side, in bytes
-    static constexpr int MMAS_PER_STAGE = kRowBytes / MMA_K_BYTES;
-    static constexpr int B_KSTEP_BYTES = (MMA_K_BYTES / T::elt) * kRowBytes;
-    // stride between k-row groups of the B swizzle atom: 8 rows (16B chunks) or 4 rows (32B)
-    static constexpr int B_SBO = T::b_layout == SMEM_SW128_32B ? 512 : 1024;
-    // 3xTF32 keeps the small hi*lo + lo*hi terms in their own accumulator next to
-    // hi*hi: each of the two TMEM buffers is then [hi*hi | corrections].
-    static constexpr int ACC_COLS = (T::split ? 2 : 1) * T::BN;
-    static constexpr int TMEM_COLS = 2 * ACC_COLS;
-    static constexpr int SMEM_BYTES = T::STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*bars*/;
-};
-
-struct __align__(8) Bars {
-    uint64_t full[4];
-    uint64_t empty[4];
-    uint64_t acc_full[2];
-    uint64_t acc_empty[2];
-    uint64_t mma_done;
-    uint32_t tmem_base;
-    int abort;
-};
-
-__device__ __forceinline__ void set_abort(Bars *b) { *reinterpret_cast<volatile int *>(&b->abort) = 1; }
-__device__ __forceinline__ bool aborted(Bars *b) { return *reinterpret_cast<volatile int *>(&b->abort) != 0; }
-
-// ------------------------------------------------------------------ epilogue helpers
-
-__device__ __forceinline__ uint16_t f32_to_bf16_rne(float f)
-{
-    uint32_t u = __float_as_uint(f);
-    if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40u);
-    u += 0x7fffu + ((u >> 16) & 1u);
-    return (uint16_t)(u >> 16);
-}
-
-// Round FP32 to the nearest TF32 value (10 explicit mantissa bits), ties to even.
-__device__ __forceinline__ float f32_to_tf32_rne(float f)
-{
-    uint32_t u = __float_as_uint(f);
-    if ((u & 0x7f800000u) == 0x7f800000u) return f;
-    u += 0xfffu + ((u >> 13) & 1u);
-    return __uint_as_float(u & 0xffffe000u);
-}
-
-__device__ __forceinline__ int8_t sat_s8(int32_t v)
-{
-    return (int8_t)(v > 127 ? 127 : (v < -128 ? -128 : v));
-}
-
-// Store one 32-column chunk of output row `row`, columns [n0, n0 + 32).
-// v holds the raw accumulator bits (FP32 or S32).
-template <int OP>
-__device__ __forceinline__ void store_chunk(const StageArgs &p, int row, int n0, uint32_t (&v)[32])
-{
-    const int N = p.N;
-    const bool full = (n0 + 32 <= N);
-    // each operand kind reaches only its own epilogues; keep the others out of its code
-    const int epi = OP == OP_BF16 ? (p.epi == EPI_BF16 ? EPI_BF16 : EPI_F32)
-                  : OP == OP_I8   ? (p.epi == EPI_S8 ? EPI_S8 : EPI_S32)
-                                  : (p.epi == EPI_TF32SPLIT ? EPI_TF32SPLIT : EPI_F32);
-    switch (epi) {
-    case EPI_F32:
-    case EPI_S32: {
-        if (row >= p.m_written) return;
-        uint32_t *c = reinterpret_cast<uint32_t *>(p.out) + (size_t)row * p.ld_out + n0;
-        if (full && ((p.ld_out & 3) == 0)) {
-#pragma unroll
-            for (int j = 0; j < 32; j += 4)
-                *reinterpret_cast<uint4 *>(c + j) = make_uint4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-        } else {
-#pragma unroll
-            for (int j = 0; j < 32; ++j)
-                if (n0 + j < N) c[j] = v[j];
-        }
-        return;
-    }
-    case EPI_BF16: {
-        uint16_t h[32];
-#pragma unroll
-        for (int j = 0; j < 32; ++j) h[j] = f32_to_bf16_rne(__uint_as_float(v[j]));
-        uint16_t *out = reinterpret_cast<uint16_t *>(p.out);
-        if (p.permute && full && row < (p.M & ~1)) {
-            // The reference stores the 2 x 32 block rows (2q, 2q+1) row-major and the
-            // next stage reads it K-pair interleaved (multigemm/src/kernel_bf16.h:6-32,
-            // :356-391): element (2q + h, c) lands at (2q + (c & 1), 16h + c / 2).
-            const int hbit = row & 1;
-            const int r0 = row - hbit;
-            uint32_t ev[8], od[8];
-#pragma unroll
-            for (int t = 0; t < 8; ++t) {
-                ev[t] = (uint32_t)h[4 * t] | ((uint32_t)h[4 * t + 2] << 16);
-                od[t] = (uint32_t)h[4 * t + 1] | ((uint32_t)h[4 * t + 3] << 16);
-            }
-            uint16_t *d0 = out + (size_t)r0 * p.ld_out + n0 + 16 * hbit;
-            uint16_t *d1 = d0 + p.ld_out;
-            *reinterpret_cast<uint4 *>(d0) = make_uint4(ev[0], ev[1], ev[2], ev[3]);
-            *reinterpret_cast<uint4 *>(d0 + 8) = make_uint4(ev[4], ev[5], ev[6], ev[7]);
-            *reinterpret_cast<uint4 *>(d1) = make_uint4(od[0], od[1], od[2], od[3]);
-            *reinterpret_cast<uint4 *>(d1 + 8) = make_uint4(od[4], od[5], od[6], od[7]);
-        } else {
-            uint16_t *d = out + (size_t)row * p.ld_out + n0;
-            if (full && ((p.ld_out & 7) == 0)) {
-                uint32_t w[16];
-#pragma unroll
-                for (int t = 0; t < 16; ++t) w[t] = (uint32_t)h[2 * t] | ((uint32_t)h[2 * t + 1] << 16);
-#pragma unroll
-                for (int t = 0; t < 16; t += 4)
-                    *reinterpret_cast<uint4 *>(d + 2 * t) = make_uint4(w[t], w[t + 1], w[t + 2], w[t + 3]);
-            } else {
-#pragma unroll
-                for (int j = 0; j < 32; ++j)
-                    if (n0 + j < N) d[j] = h[j];
-            }
-        }
-        return;
-    }
-    case EPI_S8: {
-        uint8_t b[32];
-#pragma unroll
-        for (int j = 0; j < 32; ++j) b[j] = (uint8_t)sat_s8((int32_t)v[j]);
-        uint8_t *out = reinterpret_cast<uint8_t *>(p.out);
-        const int quad_rows = (p.M / 4) * 4;
-        if (p.permute && full && row < quad_rows) {
-            // 4 x 32 blocks: stored row-major, read K-quad interleaved
-            // (multigemm/src/kernel_int8.h:6-50, :329-385): element (4q + h, c)
-            // lands at (4q + (c & 3), 8h + c / 4).
-            const int hq = row & 3;
-            const int r0 = row - hq;
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                uint32_t lo = (uint32_t)b[r] | ((uint32_t)b[r + 4] << 8) | ((uint32_t)b[r + 8] << 16) |
-                              ((uint32_t)b[r + 12] << 24);
-                uint32_t hi = (uint32_t)b[r + 16] | ((uint32_t)b[r + 20] << 8) |
-                              ((uint32_t)b[r + 24] << 16) | ((uint32_t)b[r + 28] << 24);
-                uint8_t *d = out + (size_t)(r0 + r) * p.ld_out + n0 + 8 * hq;
-                *reinterpret_cast<uint2 *>(d) = make_uint2(lo, hi);
-            }
-        } else {
-            uint8_t *d = out + (size_t)row * p.ld_out + n0;
-            if (full && ((p.ld_out & 15) == 0)) {
-                uint32_t w[8];
-#pragma unroll
-                for (int t = 0; t < 8; ++t)
-                    w[t] = (uint32_t)b[4 * t] | ((uint32_t)b[4 * t + 1] << 8) |
-                           ((uint32_t)b[4 * t + 2] << 16) | ((uint32_t)b[4 * t + 3] << 24);
-                *reinterpret_cast<uint4 *>(d) = make_uint4(w[0], w[1], w[2], w[3]);
-                *reinterpret_cast<uint4 *>(d + 16) = make_uint4(w[4], w[5], w[6], w[7]);
-            } else {
-#pragma unroll
-                for (int j = 0; j < 32; ++j)
-                    if (n0 + j < N) d[j] = b[j];
-            }
-        }
-        return;
-    }
-    case EPI_TF32SPLIT: {
-        float *hi = reinterpret_cast<float *>(p.out) + (size_t)row * p.ld_out + n0;
-        float *lo = reinterpret_cast<float *>(p.out_lo) + (size_t)row * p.ld_out + n0;
-#pragma unroll
-        for (int j = 0; j < 32; ++j) {
-            if (full || n0 + j < N) {
-                float x = __uint_as_float(v[j]);
-                float h = f32_to_tf32_rne(x);
-                hi[j] = h;
-                lo[j] = f32_to_tf32_rne(x - h);
-            }
-        }
-        return;
-    }
-    default:
-        return;
-    }
-}
 
 // ------------------------------------------------------------------ kernel
 
@@ -260,7 +33,8 @@ template <int OP>
 __global__ void __launch_bounds__(kThreads, 1)
     tc_stage_kernel(const __grid_constant__ CUtensorMap tm_w, const __grid_constant__ CUtensorMap tm_x,
                     const __grid_constant__ CUtensorMap tm_w_lo,
-                    const __grid_constant__ CUtensorMap tm_x_lo, const StageArgs p)
+                    const __grid_constant__ CUtensorMap tm_x_lo,
+                    const __grid_constant__ CUtensorMap tm_out, const StageArgs p)
 {
     using T = OpTraits<OP>;
     using G = Geometry<OP>;
@@ -270,7 +44,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
-    Bars *bars = reinterpret_cast<Bars *>(smem + S * G::STAGE_BYTES);
+    Bars *bars = reinterpret_cast<Bars *>(smem + S * G::STAGE_BYTES + G::STAGING_BYTES);
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -334,7 +108,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                     uint8_t *st = smem + s * G::STAGE_BYTES;
                     mbar_arrive_expect_tx(&bars->full[s], tx_bytes);
                     const int k0 = kb * G::BK;
-                    tma_load_2d(st, &tm_w, &bars->full[s], k0, m0);
+                    if (OP == OP_I8 && tile_has_tail(p, m0))  // INT8: tail block in tm_w_lo
+                        tma_load_2d(st, &tm_w_lo, &bars->full[s], k0, m0 - p.tail_row0);
+                    else
+                        tma_load_2d(st, &tm_w, &bars->full[s], k0, m0);
                     for (int j = 0; j < nvb; ++j)
                         tma_load_2d(st + G::A_BYTES + j * G::BOX_BYTES, &tm_x, &bars->full[s],
                                     n0 + j * G::BOX_N, k0);
@@ -490,7 +267,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
                 if (aborted(bars)) break;
             }
-        } else
+        } else {
+        uint8_t *staging = smem + S * G::STAGE_BYTES + (warp - 2) * 2 * kStageBufBytes;
+        int sbuf = 0;
         for (int t = blockIdx.x; t < num_tiles; t += gridDim.x) {
             if (!mbar_wait(&bars->acc_full[acc], acc_ph, p.status, KERR_WAIT_ACC_FULL)) {
                 set_abort(bars);
@@ -499,33 +278,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc_fence_after();
             const int m0 = (t / tiles_n) * kBM;
             const int n0 = (t % tiles_n) * BN;
-            const int row = m0 + quarter * 32 + lane;
             const uint32_t t_row = tmem_base + acc * G::ACC_COLS + ((uint32_t)(quarter * 32) << 16);
-            const bool tail = (row >= p.tail_lo && row < p.tail_hi);
-            uint32_t wq = 0;
-            if (tail) wq = *reinterpret_cast<const uint32_t *>(
-                              reinterpret_cast<const uint8_t *>(p.w) + (size_t)row * p.ld_w + p.K);
-#pragma unroll 1
-            for (int c = 0; c < BN / 32; ++c) {
-                uint32_t v[32];
-                tmem_ld_32x32b_x32(t_row + c * 32, v);
-                tmem_ld_wait();
-                const int nc = n0 + c * 32;
-                if (nc >= p.N) continue;  // whole chunk past the last column (warp-uniform)
-                if (tail) {
-                    // INT8 reference tail rows: add back weight quad 0 * activation quad 0
-                    const int8_t *x = reinterpret_cast<const int8_t *>(p.x);
-#pragma unroll
-                    for (int r = 0; r < 4; ++r) {
-                        const int a = (int)((wq >> (8 * r)) & 0xffu);
-                        const int8_t *xr = x + (size_t)r * p.ld_x + nc;
-#pragma unroll
-                        for (int j = 0; j < 32; ++j)
-                            if (nc + j < p.N) v[j] = (uint32_t)((int32_t)v[j] + a * (int32_t)xr[j]);
-                    }
-                }
-                if (row < p.M) store_chunk<OP>(p, row, nc, v);
-            }
+            drain_warp<OP, BN>(p, &tm_out, t_row, lane, m0 + quarter * 32, n0, staging, sbuf);
             tc_fence_before();
             mbar_arrive(&bars->acc_empty[acc]);
             if (++acc == 2) {
@@ -534,8 +288,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             if (aborted(bars)) break;
         }
+        }
     }
 
+    if (warp >= 2 && lane == 0) bulk_wait<0>();  // staged stores done before shared memory goes
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {
@@ -545,45 +301,220 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
-// ------------------------------------------------------------------ host side
 
-using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
-                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
-                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+// ------------------------------------------------------------------ two-CTA kernel
+//
+// Same stage, computed by CTA pairs (clusters of 2) with cta_group::2 MMAs on
+// 256 x 256 tiles: each CTA stages 128 weight rows and 128 activation columns
+// per k-block (32 KB instead of 48 KB for the same 4.2 MFLOP per CTA), which
+// is what bounds the single-CTA version (L2 -> shared memory traffic). The
+// pair's first CTA ("leader") owns the pipeline: its full barriers count the
+// bytes both CTAs load, it alone issues the MMAs, and its commits arrive on
+// the barriers of both CTAs. Each CTA's epilogue drains its own 128 TMEM
+// lanes (output rows) and arrives on the leader's accumulator-empty barrier.
 
-static EncodeTiledFn encode_fn()
+template <int OP>
+__global__ void __launch_bounds__(kThreads, 1)
+    tc_pair_kernel(const __grid_constant__ CUtensorMap tm_w, const __grid_constant__ CUtensorMap tm_x,
+                   const __grid_constant__ CUtensorMap tm_wt,
+                   const __grid_constant__ CUtensorMap tm_out, const StageArgs p)
 {
-    static EncodeTiledFn fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    });
-    return fn;
+    using T = OpTraits<OP>;
+    using G = PairGeo<OP>;
+    constexpr int S = G::STAGES;
+    constexpr int BN = G::BN;
+
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+    Bars *bars = reinterpret_cast<Bars *>(smem + S * G::STAGE_BYTES + G::STAGING_BYTES);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    const bool leader = (rank == 0);
+    const int pair = blockIdx.x >> 1;
+    const int npairs = gridDim.x >> 1;
+    const int tiles_m = (p.M + G::BM - 1) / G::BM;
+    const int tiles_n = (p.N + BN - 1) / BN;
+    const int num_tiles = tiles_m * tiles_n;
+    const int num_kb = (p.K + G::BK - 1) / G::BK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&bars->full[s], 1);
+            mbar_init(&bars->empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&bars->acc_full[a], 1);
+            mbar_init(&bars->acc_empty[a], 2 * 4);  // one arrival per epilogue warp, both CTAs
+        }
+        mbar_init(&bars->mma_done, 1);
+        bars->abort = 0;
+        fence_mbar_init();
+    }
+    if (warp == 0 && lane == 0) {
+        tma_prefetch_desc(&tm_w);
+        tma_prefetch_desc(&tm_x);
+    }
+    if (warp == 1) tmem_alloc_pair(&bars->tmem_base, G::TMEM_COLS);
+    tc_fence_before();
+    cluster_sync();  // both CTAs' barriers initialised and TMEM allocated
+    tc_fence_after();
+    const uint32_t tmem_base = bars->tmem_base;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ TMA producer (both CTAs)
+        if (lane == 0) {
+            int s = 0;
+            uint32_t ph = 0;
+            uint32_t pending = 0, pending_ph = 0;  // leader: stages with loads in flight
+            for (int t = pair; t < num_tiles; t += npairs) {
+                const int m0p = (t / tiles_n) * G::BM;
+                const int n0 = (t % tiles_n) * BN;
+                // boxes past the matrix edge are not loaded (they only feed rows or
+                // columns that are never stored); both CTAs count them the same way
+                int tx = 0, my_boxes = 0;
+                bool my_a = false;
+                for (int r = 0; r < 2; ++r) {
+                    const bool a_in = m0p + 128 * r < p.M;
+                    int nb = 0;
+                    for (int j = 0; j < G::NBOX; ++j)
+                        if (n0 + (BN / 2) * r + j * G::BOX_N < p.N) ++nb;
+                    tx += (a_in ? G::A_BYTES : 0) + nb * G::BOX_BYTES;
+                    if (r == (int)rank) {
+                        my_a = a_in;
+                        my_boxes = nb;
+                    }
+                }
+                for (int kb = 0; kb < num_kb; ++kb) {
+                    if (!mbar_wait(&bars->empty[s], ph ^ 1, p.status, KERR_WAIT_EMPTY)) {
+                        set_abort(bars);
+                        goto producer_done;
+                    }
+                    uint8_t *st = smem + s * G::STAGE_BYTES;
+                    const uint32_t full_leader = mapa_shared(smem_u32(&bars->full[s]), 0);
+                    if (leader) mbar_arrive_expect_tx(&bars->full[s], (uint32_t)tx);
+                    const int k0 = kb * G::BK;
+                    if (my_a) {
+                        const int ma = m0p + 128 * (int)rank;
+                        if (tile_has_tail(p, ma))
+                            tma_load_2d_pair(st, &tm_wt, full_leader, k0, ma - p.tail_row0);
+                        else
+                            tma_load_2d_pair(st, &tm_w, full_leader, k0, ma);
+                    }
+                    for (int j = 0; j < my_boxes; ++j)
+                        tma_load_2d_pair(st + G::A_BYTES + j * G::BOX_BYTES, &tm_x, full_leader,
+                                         n0 + (BN / 2) * (int)rank + j * G::BOX_N, k0);
+                    if (leader) {
+                        pending |= 1u << s;
+                        pending_ph = (pending_ph & ~(1u << s)) | (ph << s);
+                    }
+                    if (++s == S) {
+                        s = 0;
+                        ph ^= 1;
+                    }
+                }
+                if (aborted(bars)) break;
+            }
+        producer_done:
+            // the leader's full barriers also count the peer's bytes: once they
+            // complete, no copy of either CTA is still in flight
+            for (int st = 0; st < S; ++st)
+                if (pending & (1u << st))
+                    mbar_wait(&bars->full[st], (pending_ph >> st) & 1u, p.status, KERR_WAIT_FULL);
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer (leader only)
+        if (lane == 0 && leader) {
+            int s = 0;
+            uint32_t ph = 0;
+            int acc = 0;
+            uint32_t acc_ph = 0;
+            for (int t = pair; t < num_tiles; t += npairs) {
+                if (!mbar_wait(&bars->acc_empty[acc], acc_ph ^ 1, p.status, KERR_WAIT_ACC_EMPTY)) {
+                    set_abort(bars);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d_tmem = tmem_base + acc * BN;
+                bool ok = true;
+                for (int kb = 0; kb < num_kb; ++kb) {
+                    if (!mbar_wait(&bars->full[s], ph, p.status, KERR_WAIT_FULL)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a_addr = smem_u32(smem + s * G::STAGE_BYTES);
+                    const uint32_t b_addr = a_addr + G::A_BYTES;
+#pragma unroll
+                    for (int k = 0; k < G::MMAS_PER_STAGE; ++k) {
+                        const uint64_t ad =
+                            smem_desc(a_addr + k * G::MMA_K_BYTES, 16, 1024, SMEM_SW128);
+                        const uint64_t bd = smem_desc(b_addr + k * G::B_KSTEP_BYTES, G::BOX_BYTES,
+                                                      1024, SMEM_SW128);
+                        tc_mma_pair<T::kind>(d_tmem, ad, bd, G::idesc, (kb | k) != 0);
+                    }
+                    tc_commit_pair(&bars->empty[s], 0x3);  // stage free in both CTAs
+                    if (++s == S) {
+                        s = 0;
+                        ph ^= 1;
+                    }
+                }
+                if (!ok) {
+                    set_abort(bars);
+                    break;
+                }
+                tc_commit_pair(&bars->acc_full[acc], 0x3);  // accumulator ready in both CTAs
+                if (++acc == 2) {
+                    acc = 0;
+                    acc_ph ^= 1;
+                }
+                if (aborted(bars)) break;
+            }
+            tc_commit_pair(&bars->mma_done, 0x1);
+            mbar_wait(&bars->mma_done, 0, p.status, KERR_WAIT_FULL);
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue (warps 2..5, both CTAs)
+        const int quarter = warp & 3;
+        int acc = 0;
+        uint32_t acc_ph = 0;
+        uint8_t *staging = smem + S * G::STAGE_BYTES + (warp - 2) * 2 * kStageBufBytes;
+        int sbuf = 0;
+        for (int t = pair; t < num_tiles; t += npairs) {
+            if (!mbar_wait(&bars->acc_full[acc], acc_ph, p.status, KERR_WAIT_ACC_FULL)) {
+                set_abort(bars);
+                break;
+            }
+            tc_fence_after();
+            const int m0 = (t / tiles_n) * G::BM + 128 * (int)rank;
+            const int n0 = (t % tiles_n) * BN;
+            const uint32_t t_row = tmem_base + acc * BN + ((uint32_t)(quarter * 32) << 16);
+            drain_warp<OP, BN>(p, &tm_out, t_row, lane, m0 + quarter * 32, n0, staging, sbuf);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(mapa_shared(smem_u32(&bars->acc_empty[acc]), 0));
+            if (++acc == 2) {
+                acc = 0;
+                acc_ph ^= 1;
+            }
+            if (aborted(bars)) break;
+        }
+    }
+
+    if (warp >= 2 && lane == 0) bulk_wait<0>();  // staged stores done before shared memory goes
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();  // both CTAs done with TMEM and shared memory
+    if (warp == 1) {
+        __syncwarp();
+        tc_fence_after();
+        tmem_dealloc_pair(tmem_base, G::TMEM_COLS);
+    }
 }
 
-// Row-major rows x cols matrix with leading dimension ld (elements); box is
-// box_cols (innermost, 128 bytes) x box_rows, 128-byte swizzle, zero fill.
-static bool make_map(CUtensorMap *m, CUtensorMapDataType dt, int elt, const void *base, long rows,
-                     long cols, long ld, int box_cols, int box_rows,
-                     CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_128B)
-{
-    EncodeTiledFn enc = encode_fn();
-    if (!enc) return false;
-    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)ld * elt};
-    cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
-    cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(m, dt, 2, const_cast<void *>(base), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
-                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS;
-}
+// ------------------------------------------------------------------ launchers
 
 template <int OP>
 static cudaError_t launch_op(const StageArgs &a, int num_sms, cudaStream_t s)
@@ -600,7 +531,11 @@ static cudaError_t launch_op(const StageArgs &a, int num_sms, cudaStream_t s)
     if (!make_map(&tw, dt, T::elt, a.w, a.M, a.K, a.ld_w, G::BK, kBM)) return cudaErrorInvalidValue;
     if (!make_map(&tx, dt, T::elt, a.x, a.K, a.N, a.ld_x, G::BOX_N, G::BK, bswz))
         return cudaErrorInvalidValue;
-    if (T::split) {
+    if (OP == OP_I8 && a.tail_hi > a.tail_lo) {
+        if (!make_map(&twl, dt, T::elt, a.w_tail, a.M - a.tail_row0, a.K, a.ld_w_tail, G::BK, kBM))
+            return cudaErrorInvalidValue;
+        txl = tx;
+    } else if (T::split) {
         if (!make_map(&twl, dt, T::elt, a.w_lo, a.M, a.K, a.ld_w, G::BK, kBM)) return cudaErrorInvalidValue;
         if (!make_map(&txl, dt, T::elt, a.x_lo, a.K, a.N, a.ld_x, G::BOX_N, G::BK, bswz))
             return cudaErrorInvalidValue;
@@ -619,16 +554,85 @@ static cudaError_t launch_op(const StageArgs &a, int num_sms, cudaStream_t s)
     }
     const int tiles = ((a.M + kBM - 1) / kBM) * ((a.N + T::BN - 1) / T::BN);
     const int grid = tiles < num_sms ? tiles : num_sms;
-    tc_stage_kernel<OP><<<grid, kThreads, G::SMEM_BYTES, s>>>(tw, tx, twl, txl, a);
+    StageArgs b = a;
+    CUtensorMap to;
+    b.tma_store = (!T::split && make_out_map(&to, b)) ? 1 : 0;
+    if (!b.tma_store) to = tw;
+    tc_stage_kernel<OP><<<grid, kThreads, G::SMEM_BYTES, s>>>(tw, tx, twl, txl, to, b);
     return cudaGetLastError();
+}
+
+template <int OP>
+static cudaError_t launch_pair(const StageArgs &a, int num_sms, cudaStream_t s)
+{
+    using T = OpTraits<OP>;
+    using G = PairGeo<OP>;
+    CUtensorMapDataType dt = OP == OP_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                           : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+    CUtensorMap tw, tx, twt;
+    if (!make_map(&tw, dt, T::elt, a.w, a.M, a.K, a.ld_w, G::BK, 128)) return cudaErrorInvalidValue;
+    if (!make_map(&tx, dt, T::elt, a.x, a.K, a.N, a.ld_x, G::BOX_N, G::BK)) return cudaErrorInvalidValue;
+    if (a.tail_hi > a.tail_lo) {
+        if (!make_map(&twt, dt, T::elt, a.w_tail, a.M - a.tail_row0, a.K, a.ld_w_tail, G::BK, 128))
+            return cudaErrorInvalidValue;
+    } else {
+        twt = tw;
+    }
+    static unsigned long long attr_set = 0;
+    static int max_pairs[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = G::SMEM_BYTES;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (!(attr_set & (1ull << (dev & 63)))) {
+        cudaError_t e = cudaFuncSetAttribute(tc_pair_kernel<OP>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        int clusters = 0;
+        cfg.gridDim = dim3(2 * (num_sms / 2));
+        e = cudaOccupancyMaxActiveClusters(&clusters, tc_pair_kernel<OP>, &cfg);
+        if (e != cudaSuccess || clusters < 1) {
+            cudaGetLastError();
+            clusters = num_sms / 2;
+        }
+        max_pairs[dev & 63] = clusters;
+        attr_set |= 1ull << (dev & 63);
+    }
+    const int tiles = ((a.M + G::BM - 1) / G::BM) * ((a.N + G::BN - 1) / G::BN);
+    const int pairs = tiles < max_pairs[dev & 63] ? tiles : max_pairs[dev & 63];
+    cfg.gridDim = dim3(2 * pairs);
+    StageArgs b = a;
+    CUtensorMap to;
+    b.tma_store = make_out_map(&to, b) ? 1 : 0;
+    if (!b.tma_store) to = tw;
+    return cudaLaunchKernelEx(&cfg, tc_pair_kernel<OP>, tw, tx, twt, to, b);
+}
+
+// Two-CTA tiles for BF16 and INT8 unless FG_CTA_PAIR=0.
+static bool use_pairs()
+{
+    static const bool on = [] {
+        const char *v = getenv("FG_CTA_PAIR");
+        return !(v && v[0] == '0');
+    }();
+    return on;
 }
 
 cudaError_t launch_tc_stage(const StageArgs &a, int num_sms, cudaStream_t s)
 {
     if (a.M <= 0 || a.N <= 0 || a.K <= 0) return cudaErrorInvalidValue;
     switch (a.op) {
-    case OP_BF16: return launch_op<OP_BF16>(a, num_sms, s);
-    case OP_I8: return launch_op<OP_I8>(a, num_sms, s);
+    case OP_BF16: return use_pairs() ? launch_pair<OP_BF16>(a, num_sms, s) : launch_op<OP_BF16>(a, num_sms, s);
+    case OP_I8: return use_pairs() ? launch_pair<OP_I8>(a, num_sms, s) : launch_op<OP_I8>(a, num_sms, s);
     case OP_TF32X3: return launch_op<OP_TF32X3>(a, num_sms, s);
     default: return cudaErrorInvalidValue;
     }

@@ -35,13 +35,27 @@ struct StageArgs {
     long ld_out;
     int permute;       // 1: apply the reference's panel permutation (EPI_BF16 / EPI_S8)
     int m_written;     // rows >= m_written are not stored (INT8 reference semantics)
-    int tail_lo;       // INT8 reference tail rows [tail_lo, tail_hi): weights pre-shifted,
-    int tail_hi;       //   first k-quad kept at w[m * ld_w + K .. +3], added in the epilogue
+    int tail_lo;       // INT8 reference tail rows [tail_lo, tail_hi): their weights come from
+    int tail_hi;       //   w_tail (rows tail_row0 .. M-1, pre-shifted by one k-quad, first
+    const void *w_tail;//   quad kept at [K, K + 4) for the epilogue's correction term)
+    long ld_w_tail;
+    int tail_row0;
     int kchunk;        // TF32X3: k-blocks (of 32) per FP32 promotion of the partial sum
+    int tma_store;     // set by the launchers: the epilogue writes `out` with TMA bulk stores
     int *status;       // device status word (0 = ok)
 };
 
 cudaError_t launch_tc_stage(const StageArgs &a, int num_sms, cudaStream_t s);
+
+// A whole BF16 or INT8 chain (stages[0..n) with the same op and N) in one
+// cooperative persistent launch; `done` holds n * ceil(N / 256) zeroed ints.
+// Returns cudaErrorNotSupported (nothing launched) where the device cannot
+// run it; the caller then launches the stages one by one.
+// trace (optional, else null): chain_trace_fields() %globaltimer stamps per (item, CTA).
+cudaError_t launch_tc_chain(const StageArgs *stages, int n, int *done, int *status,
+                            unsigned long long *trace, int num_sms, cudaStream_t s);
+int chain_max_stages();
+int chain_trace_fields();
 
 // Plain FP32 SGEMM on CUDA cores: C = A * B, one FMA per k in increasing k;
 // with kblock > 0 each block of kblock k is summed from zero and added to C.
@@ -58,14 +72,14 @@ cudaError_t launch_ffma_sgemm(const FfmaArgs &a, int num_sms, cudaStream_t s);
 cudaError_t launch_split_tf32(const float *in, long ld_in, float *hi, float *lo, long ld_out,
                               long rows, long cols, cudaStream_t s);
 
-// INT8 reference-semantics weight preparation: copies W (M x K, ld_in) into
-// dst (ld_out >= K + 4), shifting rows [tail_lo, tail_hi) left by one k-quad
+// INT8 weight preparation: copies W (M x K, ld_in) into dst (ld_out >= K + 4,
+// a multiple of 16), shifting rows [tail_lo, tail_hi) left by one k-quad
 // (zero-filling the last quad) and keeping their first quad at [K, K + 4).
 cudaError_t launch_prep_int8_weights(const int8_t *src, long ld_in, uint8_t *dst, long ld_out,
                                      long M, long K, long tail_lo, long tail_hi,
                                      cudaStream_t s);
 
-// Copy of a rows x cols byte matrix between leading dimensions (device to device).
+// Fill `count` 32-bit words with `value`.
 cudaError_t launch_fill_u32(uint32_t *dst, size_t count, uint32_t value, cudaStream_t s);
 
 }  // namespace fg
