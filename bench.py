@@ -68,6 +68,14 @@ def load_peaks():
 
 # ---------------------------------------------------------------- clocks (NVML, read only)
 
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
 class ClockSampler:
     """Samples SM clock and clock-event reasons of one GPU every 10 ms."""
 
@@ -324,38 +332,58 @@ def main():
     torch.cuda.synchronize(dev)
     fg.sync()
 
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    sampler = ClockSampler(torch.cuda.current_device() if world == 1 else local_rank)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    l0 = fg.kernel_launches()
-    fg.profile_begin()
-    with sampler:
-        t_wall = time.perf_counter()
-        for i in range(args.steps):
-            flush.fill_(i & 0xFF)
-            starts[i].record()
-            step()
-            stops[i].record()
+    def timed_steps(sampler=None):
+        """Exactly args.steps steps, each bracketed by CUDA events on torch's
+        stream (the library orders its own stream after it and back), L2
+        flushed between steps outside the events. Returns (sum of step ms,
+        wall seconds, our kernel launches, profile of the stage kernel)."""
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        if dist:
+            dist.barrier()
         torch.cuda.synchronize(dev)
-        fg.sync()
-        t_wall = time.perf_counter() - t_wall
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    fg.profile_end()
-    launches = fg.kernel_launches() - l0
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
-    total_ms = sum(step_ms)
-    k_ms, k_n, k_fl = fg.profile_query(kind)
+        l0 = fg.kernel_launches()
+        fg.profile_begin()
+        ctx = sampler if sampler is not None else _Null()
+        with ctx:
+            t_wall = time.perf_counter()
+            for i in range(args.steps):
+                flush.fill_(i & 0xFF)
+                starts[i].record()
+                step()
+                stops[i].record()
+            torch.cuda.synchronize(dev)
+            fg.sync()
+            t_wall = time.perf_counter() - t_wall
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        fg.profile_end()
+        prof = fg.profile_query(kind)
+        return (sum(s.elapsed_time(e) for s, e in zip(starts, stops)), t_wall,
+                fg.kernel_launches() - l0, prof)
+
+    sampler = ClockSampler(torch.cuda.current_device() if world == 1 else local_rank)
+    total_ms, t_wall, launches, (k_ms, k_n, k_fl) = timed_steps(sampler)
+
+    # the same steps through the plain per-GEMM path (one launch per GEMM)
+    per_gemm = None
+    if dt != "f32":
+        fg.set_chain_mode("per_gemm")
+        for _ in range(max(args.warmup, 3)):
+            step()
+        pg_ms, _, pg_launches, _ = timed_steps()
+        fg.set_chain_mode("fused")
+        per_gemm = (pg_ms, pg_launches)
 
     # max over ranks
     if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        t = torch.tensor([total_ms, per_gemm[0] if per_gemm else 0.0], dtype=torch.float64,
+                         device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = float(t[0].item())
+        if per_gemm:
+            per_gemm = (float(t[1].item()), per_gemm[1])
     step_flops = flops_of(N, K1, Ms)
     value = world * step_flops * args.steps / (total_ms / 1e3) / 1e12
 
@@ -422,7 +450,8 @@ def main():
                 "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved and peak else None,
                 "traffic": traffic.get("bytes_per_launch") if traffic else None,
-                "kernel": "fg::tc_stage_kernel" if dt != "f32" else "fg::ffma_sgemm_kernel",
+                "kernel": ("fg::tc_chain_kernel (whole chain, one launch)" if dt != "f32"
+                           else "fg::ffma_sgemm_kernel"),
                 "launches_timed": k_n, "avg_launch_us": 1e3 * k_ms / k_n if k_n else None,
                 "peak_source": f"{peak_name}; {peak_src}"}
 
@@ -435,6 +464,13 @@ def main():
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps,
                     "api": "flashgemm_multi_*/LibShalom_sgemm_mp, pinned host buffers"},
             "roofline": roofline, "wall_s_timed_region": t_wall}
+    if per_gemm:
+        pg_value = world * step_flops * args.steps / (per_gemm[0] / 1e3) / 1e12
+        line["per_gemm"] = {"value": pg_value, "unit": "TFLOP/s",
+                            "ms_per_step": per_gemm[0] / args.steps,
+                            "launches": per_gemm[1],
+                            "path": "one tensor-core launch per GEMM (FG_CHAIN_PER_GEMM)"}
+        line["fused_vs_per_gemm"] = value / pg_value
     if world == 1:
         tf, descr, _ = time_cpu(args.workload, budget_s=args.cpu_budget)
         line["cpu_baseline"] = dict(descr, value=tf, unit="TFLOP/s")

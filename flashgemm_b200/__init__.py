@@ -108,6 +108,17 @@ def set_sgemm_algo(algo):
     lib().fg_set_sgemm_algo({"ffma": FG_F32_FFMA, "3xtf32": FG_F32_3XTF32}.get(algo, algo))
 
 
+FG_CHAIN_FUSED, FG_CHAIN_PER_GEMM = 0, 1
+
+
+def set_chain_mode(mode):
+    lib().fg_set_chain_mode({"fused": FG_CHAIN_FUSED, "per_gemm": FG_CHAIN_PER_GEMM}.get(mode, mode))
+
+
+def get_chain_mode():
+    return lib().fg_get_chain_mode()
+
+
 def sync():
     st = lib().fg_sync()
     if st != FG_OK:

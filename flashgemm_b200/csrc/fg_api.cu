@@ -243,7 +243,7 @@ size_t chain_scratch(int dtype, int algo, long N, int n, const long *M, const lo
         if (getenv("FG_TRACE_DIR")) {  // per-tile timeline of the fused kernel
             size_t items = 0;
             for (int i = 0; i < n; ++i) items += (size_t)((M[i] + 255) / 256) * ((N + 255) / 256);
-            s += carve_size(items * 2 * 9 * 8);
+            s += carve_size(items * 2 * 10 * 8);
         }
     }
     if (dtype == FG_DT_INT8) {
@@ -303,13 +303,16 @@ double gemm_flops(long M, long N, long K) { return 2.0 * (double)M * (double)N *
 
 // Whole chain in one fused launch when possible (FG_FUSED=0 turns it off),
 // else one tensor-core launch per stage: the per-GEMM path.
+std::atomic<int> g_chain_mode{-1};
 bool fused_enabled()
 {
-    static const bool on = [] {
+    int m = g_chain_mode.load();
+    if (m < 0) {
         const char *v = getenv("FG_FUSED");
-        return !(v && v[0] == '0');
-    }();
-    return on;
+        m = (v && v[0] == '0') ? FG_CHAIN_PER_GEMM : FG_CHAIN_FUSED;
+        g_chain_mode.store(m);
+    }
+    return m == FG_CHAIN_FUSED;
 }
 bool g_fused_unsupported[64];
 
@@ -349,7 +352,7 @@ int launch_stages(DevCtx *c, int kind, std::vector<StageArgs> &stages, long N)
             snprintf(path, sizeof path, "%s/chain_trace_%d.csv", trace_dir, seq++);
             if (FILE *f = fopen(path, "w")) {
                 fprintf(f, "item,cta,sm,prod_start,dep_done,prod_end,mma_start,mma_end,epi_start,"
-                           "epi_end\n");
+                           "epi_issued,epi_end\n");
                 const int nf = chain_trace_fields();
                 for (size_t r = 0; r < trace_words / nf; ++r) {
                     fprintf(f, "%zu,%zu", r / 2, r % 2);
@@ -517,6 +520,8 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
         const void *x = b.p;
         long ldx = b.ld;
         std::vector<StageArgs> stages;
+        PrepJobs jobs;
+        jobs.n = 0;
         for (int i = 0; i < n; ++i) {
             const long Mi = M[i], Ki = K[i];
             // reference tail rows (multigemm/src/kernel_int8.h:771-1057): only with
@@ -548,12 +553,14 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             if (tail_hi > tail_lo) {
                 const long row0 = (tail_lo / 256) * 256;
                 uint8_t *wt = (uint8_t *)arena_take(c, (size_t)(Mi - row0) * ldw);
-                int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 tail-row prep", [&] {
-                    return launch_prep_int8_weights((const int8_t *)a[i].p + row0 * a[i].ld,
-                                                    a[i].ld, wt, ldw, Mi - row0, Ki,
-                                                    tail_lo - row0, tail_hi - row0, c->stream);
-                });
-                if (st) return st;
+                if (jobs.n == 8) {  // flush a full batch
+                    int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 tail-row prep",
+                                        [&] { return launch_prep_int8_jobs(jobs, c->stream); });
+                    if (st) return st;
+                    jobs.n = 0;
+                }
+                jobs.job[jobs.n++] = PrepJob{(const int8_t *)a[i].p + row0 * a[i].ld, a[i].ld, wt, ldw,
+                                             Mi - row0, Ki, tail_lo - row0, tail_hi - row0};
                 s.w_tail = wt;
                 s.ld_w_tail = ldw;
                 s.tail_row0 = (int)row0;
@@ -573,6 +580,11 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             stages.push_back(s);
             x = s.out;
             ldx = s.ld_out;
+        }
+        if (jobs.n) {  // all tail blocks of the chain in one launch
+            int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 tail-row prep",
+                                [&] { return launch_prep_int8_jobs(jobs, c->stream); });
+            if (st) return st;
         }
         return launch_stages(c, FG_PK_TC_I8, stages, N);
     }
@@ -835,6 +847,11 @@ FG_EXPORT void fg_set_f32_algo(int a) { g_f32.store(a == FG_F32_FFMA ? FG_F32_FF
 FG_EXPORT int fg_get_f32_algo(void) { return f32_algo(); }
 FG_EXPORT void fg_set_sgemm_algo(int a) { g_sgemm.store(a == FG_F32_3XTF32 ? FG_F32_3XTF32 : FG_F32_FFMA); }
 FG_EXPORT int fg_get_sgemm_algo(void) { return sgemm_algo(); }
+FG_EXPORT void fg_set_chain_mode(int mode)
+{
+    g_chain_mode.store(mode == FG_CHAIN_PER_GEMM ? FG_CHAIN_PER_GEMM : FG_CHAIN_FUSED);
+}
+FG_EXPORT int fg_get_chain_mode(void) { return fused_enabled() ? FG_CHAIN_FUSED : FG_CHAIN_PER_GEMM; }
 FG_EXPORT unsigned long long fg_kernel_launches(void) { return g_launches.load(); }
 FG_EXPORT const char *fg_version(void) { return "flashgemm-b200 0.1 (sm_100a)"; }
 

@@ -96,6 +96,57 @@ cudaError_t launch_prep_int8_weights(const int8_t *src, long ld_in, uint8_t *dst
     return cudaGetLastError();
 }
 
+// Several preparations in one launch (blockIdx.y = job).
+__global__ void prep_int8_jobs_kernel(const PrepJob *__restrict__ jobs_unused, PrepJobs jobs)
+{
+    const PrepJob &j = jobs.job[blockIdx.y];
+    const long per_row = j.ld_out / 16;
+    const long total = j.M * per_row;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+         i += (long)gridDim.x * blockDim.x) {
+        const long m = i / per_row, k0 = (i - m * per_row) * 16;
+        const uint8_t *row = reinterpret_cast<const uint8_t *>(j.src) + m * j.ld_in;
+        const bool tail = (m >= j.tail_lo && m < j.tail_hi);
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint32_t word = 0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const long k = k0 + 4 * q + b;
+                uint8_t v = 0;
+                if (tail) {
+                    if (k < j.K - 4)
+                        v = row[k + 4];
+                    else if (k >= j.K && k < j.K + 4)
+                        v = row[k - j.K];
+                } else if (k < j.K) {
+                    v = row[k];
+                }
+                word |= (uint32_t)v << (8 * b);
+            }
+            w[q] = word;
+        }
+        *reinterpret_cast<uint4 *>(j.dst + m * j.ld_out + k0) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+cudaError_t launch_prep_int8_jobs(const PrepJobs &jobs, cudaStream_t s)
+{
+    if (jobs.n <= 0) return cudaSuccess;
+    long most = 0;
+    for (int i = 0; i < jobs.n; ++i) {
+        if (jobs.job[i].ld_out % 16) return cudaErrorInvalidValue;
+        const long t = jobs.job[i].M * (jobs.job[i].ld_out / 16);
+        most = t > most ? t : most;
+    }
+    long blocks = (most + 255) / 256;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    if (blocks < 1) blocks = 1;
+    prep_int8_jobs_kernel<<<dim3((unsigned)blocks, jobs.n), 256, 0, s>>>(nullptr, jobs);
+    return cudaGetLastError();
+}
+
 __global__ void fill_u32_kernel(uint32_t *dst, size_t count, uint32_t value)
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;

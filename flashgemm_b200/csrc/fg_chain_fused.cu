@@ -92,7 +92,7 @@ __device__ __forceinline__ void decode_item(const ChainParams &P, int t, int &st
 
 // Trace record of one (item, CTA): where the time of a fused chain goes.
 enum { TR_SM = 0, TR_PROD_START, TR_DEP_DONE, TR_PROD_END, TR_MMA_START, TR_MMA_END, TR_EPI_START,
-       TR_EPI_END, kTraceFields };
+       TR_EPI_ISSUED, TR_EPI_END, kTraceFields };
 
 __device__ __forceinline__ void trace_put(const ChainParams &P, int t, uint32_t rank, int f,
                                           unsigned long long v)
@@ -325,6 +325,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
             __syncwarp();
             if (lane == 0) {
                 mbar_arrive_cluster(mapa_shared(smem_u32(&bars->acc_empty[acc]), 0));
+                if (quarter == 0) trace_put(P, t, rank, TR_EPI_ISSUED, globaltimer_ns());
                 // this warp's part of the tile is in memory: release it to the next stage
                 bulk_wait<0>();
                 fence_proxy_async_global();

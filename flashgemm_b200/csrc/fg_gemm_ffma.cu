@@ -3,29 +3,34 @@
 // Each output is one FP32 fused multiply-add per k in increasing k, the
 // arithmetic of the reference's vfmadd231ps register tiles
 // (singlegemm/src/kernel.h:8, multigemm/src/kernel_f32.h:3), so results are
-// bit-identical to the reference's. With kblock > 0, K is cut into blocks of
-// kblock: each block is summed from zero and then added into the result, as
-// singlegemm's GEMM_K = 2048 blocking does (singlegemm/src/NN_mp.h:13 and its
-// ADD_C step, singlegemm/src/kernel.h:384-400).
+// bit-identical to the reference's. With kblock > 0 and K > kblock, K is cut
+// into blocks of kblock: each block is summed from zero and then added into
+// the result, as singlegemm's GEMM_K = 2048 blocking does
+// (singlegemm/src/NN_mp.h:13 and its ADD_C step, singlegemm/src/kernel.h:384-400).
 //
-// Tiling: BM x BN block tile, BK = 8, TM x TN outputs per thread; A is staged
-// transposed (k-major) and B as is, double-buffered in shared memory with the
-// next tile prefetched into registers while the current one is consumed.
+// Tiling: BM x BN block tile, BK-deep k slices, TM x TN outputs per thread
+// held as float4 fragments spread over the tile (rows ty*4 + i*BM/(TM/4),
+// columns tx*4 + j*BN/(TN/4)) so that a warp's float4 shared-memory reads fall
+// on distinct banks; A is staged transposed (k-major) and B as is,
+// double-buffered in shared memory with the next slice prefetched into
+// registers while the current one is consumed.
 #include <cuda_runtime.h>
+
+#include <cstdlib>
 
 #include "fg_kernels.h"
 
 namespace fg {
 
-template <int BM, int BN, int TM, int TN, bool VEC>
+template <int BM, int BN, int BK, int TM, int TN, bool VEC, bool KSPLIT>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN))
     ffma_sgemm_kernel(const FfmaArgs p)
 {
-    constexpr int BK = 8;
     constexpr int NT = (BM / TM) * (BN / TN);
-    constexpr int A_LOADS = BM * BK / NT;  // elements per thread per tile
+    constexpr int A_LOADS = BM * BK / NT;  // elements per thread per slice
     constexpr int B_LOADS = BK * BN / NT;
     static_assert(A_LOADS % 4 == 0 && B_LOADS % 4 == 0, "vector tiling");
+    static_assert(TM % 4 == 0 && TN % 4 == 0, "float4 fragments");
     __shared__ __align__(16) float As[2][BK][BM];
     __shared__ __align__(16) float Bs[2][BK][BN];
 
@@ -36,18 +41,20 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
     const int n0 = blockIdx.x * BN;
     const int M = p.M, N = p.N, K = p.K;
 
-    // Load mapping. A: thread handles A_LOADS consecutive k of one row;
-    // B: thread handles B_LOADS consecutive n of one k row.
-    constexpr int A_TPR = BK / A_LOADS;  // threads per A row
+    // A: a thread loads A_LOADS consecutive k of one row; B: B_LOADS consecutive n of one k row.
+    constexpr int A_TPR = BK / A_LOADS;
     const int a_row = tid / A_TPR;
     const int a_k = (tid % A_TPR) * A_LOADS;
     constexpr int B_TPR = BN / B_LOADS;
     const int b_row = tid / B_TPR;
     const int b_n = (tid % B_TPR) * B_LOADS;
 
+    // Fragment placement: rows ty*4 + {0..3} + i*(BM/2) for the two halves of TM,
+    // columns tx*4 + {0..3} + j*(BN/2) for the two halves of TN.
+    constexpr int HM = TM / 4, HN = TN / 4;  // float4 fragments per thread per dimension
     float ra[A_LOADS], rb[B_LOADS];
 
-    auto load_tile = [&](int k0) {
+    auto load_slice = [&](int k0) {
         const int gm = m0 + a_row;
 #pragma unroll
         for (int v = 0; v < A_LOADS; v += 4) {
@@ -75,7 +82,7 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
             }
         }
     };
-    auto store_tile = [&](int buf) {
+    auto store_slice = [&](int buf) {
 #pragma unroll
         for (int v = 0; v < A_LOADS; ++v) As[buf][a_k + v][a_row] = ra[v];
 #pragma unroll
@@ -85,8 +92,8 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
     };
 
     float acc[TM][TN];
-    float sum[TM][TN];
-    const int kblock = (p.kblock > 0 && p.kblock < K) ? p.kblock : K;
+    float sum[KSPLIT ? TM : 1][KSPLIT ? TN : 1];
+    const int kblock = (KSPLIT && p.kblock > 0 && p.kblock < K) ? p.kblock : K;
 
     for (int kb0 = 0; kb0 < K; kb0 += kblock) {
         const int kb1 = min(kb0 + kblock, K);
@@ -95,27 +102,51 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
 #pragma unroll
             for (int j = 0; j < TN; ++j) acc[i][j] = 0.f;
 
-        load_tile(kb0);
-        store_tile(0);
+        load_slice(kb0);
+        store_slice(0);
         __syncthreads();
         int buf = 0;
         for (int k0 = kb0; k0 < kb1; k0 += BK) {
             const bool more = k0 + BK < kb1;
-            if (more) load_tile(k0 + BK);
+            if (more) load_slice(k0 + BK);
+            // a slice past K holds zeros for both operands; skip those k so that
+            // no extra rounding step touches the sum
             const int kend = min(BK, kb1 - k0);
+            if (kend == BK) {
 #pragma unroll
-            for (int kk = 0; kk < BK; ++kk) {
-                if (kk < kend) {
+                for (int kk = 0; kk < BK; ++kk) {
                     float a[TM], b[TN];
 #pragma unroll
-                    for (int i = 0; i < TM; i += 4) {
-                        float4 t = *reinterpret_cast<const float4 *>(&As[buf][kk][ty * TM + i]);
-                        a[i] = t.x; a[i + 1] = t.y; a[i + 2] = t.z; a[i + 3] = t.w;
+                    for (int i = 0; i < HM; ++i) {
+                        float4 t = *reinterpret_cast<const float4 *>(
+                            &As[buf][kk][ty * 4 + i * (BM / HM)]);
+                        a[4 * i] = t.x; a[4 * i + 1] = t.y; a[4 * i + 2] = t.z; a[4 * i + 3] = t.w;
                     }
 #pragma unroll
-                    for (int j = 0; j < TN; j += 4) {
-                        float4 t = *reinterpret_cast<const float4 *>(&Bs[buf][kk][tx * TN + j]);
-                        b[j] = t.x; b[j + 1] = t.y; b[j + 2] = t.z; b[j + 3] = t.w;
+                    for (int j = 0; j < HN; ++j) {
+                        float4 t = *reinterpret_cast<const float4 *>(
+                            &Bs[buf][kk][tx * 4 + j * (BN / HN)]);
+                        b[4 * j] = t.x; b[4 * j + 1] = t.y; b[4 * j + 2] = t.z; b[4 * j + 3] = t.w;
+                    }
+#pragma unroll
+                    for (int i = 0; i < TM; ++i)
+#pragma unroll
+                        for (int j = 0; j < TN; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+                }
+            } else {
+                for (int kk = 0; kk < kend; ++kk) {
+                    float a[TM], b[TN];
+#pragma unroll
+                    for (int i = 0; i < HM; ++i) {
+                        float4 t = *reinterpret_cast<const float4 *>(
+                            &As[buf][kk][ty * 4 + i * (BM / HM)]);
+                        a[4 * i] = t.x; a[4 * i + 1] = t.y; a[4 * i + 2] = t.z; a[4 * i + 3] = t.w;
+                    }
+#pragma unroll
+                    for (int j = 0; j < HN; ++j) {
+                        float4 t = *reinterpret_cast<const float4 *>(
+                            &Bs[buf][kk][tx * 4 + j * (BN / HN)]);
+                        b[4 * j] = t.x; b[4 * j + 1] = t.y; b[4 * j + 2] = t.z; b[4 * j + 3] = t.w;
                     }
 #pragma unroll
                     for (int i = 0; i < TM; ++i)
@@ -124,75 +155,109 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
                 }
             }
             if (more) {
-                store_tile(buf ^ 1);
+                store_slice(buf ^ 1);
                 __syncthreads();
                 buf ^= 1;
             }
         }
-        __syncthreads();  // buffers are refilled by the next K block
-        if (kb0 == 0) {
+        if constexpr (KSPLIT) {
+            __syncthreads();  // buffers are refilled by the next K block
+            if (kb0 == 0) {
 #pragma unroll
-            for (int i = 0; i < TM; ++i)
+                for (int i = 0; i < TM; ++i)
 #pragma unroll
-                for (int j = 0; j < TN; ++j) sum[i][j] = acc[i][j];
-        } else {
+                    for (int j = 0; j < TN; ++j) sum[i][j] = acc[i][j];
+            } else {
 #pragma unroll
-            for (int i = 0; i < TM; ++i)
+                for (int i = 0; i < TM; ++i)
 #pragma unroll
-                for (int j = 0; j < TN; ++j) sum[i][j] = sum[i][j] + acc[i][j];
+                    for (int j = 0; j < TN; ++j) sum[i][j] = sum[i][j] + acc[i][j];
+            }
         }
     }
     if (K == 0) {
 #pragma unroll
         for (int i = 0; i < TM; ++i)
 #pragma unroll
-            for (int j = 0; j < TN; ++j) sum[i][j] = 0.f;
+            for (int j = 0; j < TN; ++j) acc[i][j] = 0.f;
     }
 
 #pragma unroll
     for (int i = 0; i < TM; ++i) {
-        const int gm = m0 + ty * TM + i;
+        const int gm = m0 + ty * 4 + (i / 4) * (BM / HM) + (i % 4);
         if (gm >= M) continue;
         float *c = p.C + (size_t)gm * p.ldc;
 #pragma unroll
-        for (int j = 0; j < TN; j += 4) {
-            const int gn = n0 + tx * TN + j;
+        for (int j = 0; j < HN; ++j) {
+            const int gn = n0 + tx * 4 + j * (BN / HN);
+            float r[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if constexpr (KSPLIT)
+                    r[u] = K > 0 ? sum[i][4 * j + u] : 0.f;
+                else
+                    r[u] = acc[i][4 * j + u];
+            }
             if (VEC && gn + 3 < N) {
-                *reinterpret_cast<float4 *>(c + gn) =
-                    make_float4(sum[i][j], sum[i][j + 1], sum[i][j + 2], sum[i][j + 3]);
+                *reinterpret_cast<float4 *>(c + gn) = make_float4(r[0], r[1], r[2], r[3]);
             } else {
 #pragma unroll
                 for (int u = 0; u < 4; ++u)
-                    if (gn + u < N) c[gn + u] = sum[i][j + u];
+                    if (gn + u < N) c[gn + u] = r[u];
             }
         }
     }
 }
 
-template <int BM, int BN, int TM, int TN>
+template <int BM, int BN, int BK, int TM, int TN>
 static cudaError_t launch_cfg(const FfmaArgs &a, bool vec, cudaStream_t s)
 {
     dim3 grid((a.N + BN - 1) / BN, (a.M + BM - 1) / BM);
     dim3 block((BM / TM) * (BN / TN));
-    if (vec)
-        ffma_sgemm_kernel<BM, BN, TM, TN, true><<<grid, block, 0, s>>>(a);
-    else
-        ffma_sgemm_kernel<BM, BN, TM, TN, false><<<grid, block, 0, s>>>(a);
+    const bool split = a.kblock > 0 && a.kblock < a.K;
+    if (vec) {
+        if (split)
+            ffma_sgemm_kernel<BM, BN, BK, TM, TN, true, true><<<grid, block, 0, s>>>(a);
+        else
+            ffma_sgemm_kernel<BM, BN, BK, TM, TN, true, false><<<grid, block, 0, s>>>(a);
+    } else {
+        if (split)
+            ffma_sgemm_kernel<BM, BN, BK, TM, TN, false, true><<<grid, block, 0, s>>>(a);
+        else
+            ffma_sgemm_kernel<BM, BN, BK, TM, TN, false, false><<<grid, block, 0, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_ffma_sgemm(const FfmaArgs &a, int num_sms, cudaStream_t s)
 {
     if (a.M <= 0 || a.N <= 0) return cudaSuccess;
+    if (a.kblock > 0 && a.kblock % 16) return cudaErrorInvalidValue;  // K blocks end on slices
     const bool vec = ((a.lda | a.ldb | a.ldc) % 4 == 0) &&
                      (((uintptr_t)a.A | (uintptr_t)a.B | (uintptr_t)a.C) % 16 == 0);
-    // Largest tile that still gives every SM a block; small problems drop to
-    // 64 x 64 tiles so that more of the 148 SMs have work.
-    const long tiles128 = (long)((a.M + 127) / 128) * ((a.N + 127) / 128);
-    if (tiles128 >= num_sms) return launch_cfg<128, 128, 8, 8>(a, vec, s);
-    const long tiles64 = (long)((a.M + 127) / 128) * ((a.N + 63) / 64);
-    if (tiles64 >= num_sms) return launch_cfg<128, 64, 8, 8>(a, vec, s);
-    return launch_cfg<64, 64, 4, 8>(a, vec, s);
+    // FG_FFMA_CFG forces one tile configuration (0..7). By default 128 x 128 x 16
+    // tiles when there are at least two per SM, else 64 x 64 x 16 (measured on
+    // B200: 1024^3 25.9 TFLOP/s with 64 x 64 vs 17.8 with 128 x 128; 4096^3 38.4
+    // with 128 x 128 x 16).
+    static const int forced = [] {
+        const char *v = getenv("FG_FFMA_CFG");
+        return v ? atoi(v) : -1;
+    }();
+    const long t128 = (long)((a.M + 127) / 128) * ((a.N + 127) / 128);
+    const long t12864 = (long)((a.M + 127) / 128) * ((a.N + 63) / 64);
+    int cfg = forced;
+    if (cfg < 0) cfg = t128 >= 2l * num_sms ? 5 : 2;
+    (void)t12864;
+    switch (cfg) {
+    case 0: return launch_cfg<128, 128, 8, 8, 8>(a, vec, s);   // 256 threads
+    case 1: return launch_cfg<128, 64, 8, 8, 8>(a, vec, s);    // 128 threads
+    case 2: return launch_cfg<64, 64, 16, 4, 8>(a, vec, s);    // 128 threads
+    case 3: return launch_cfg<64, 128, 8, 8, 8>(a, vec, s);    // 128 threads
+    case 4: return launch_cfg<64, 64, 32, 4, 8>(a, vec, s);    // 128 threads
+    case 5: return launch_cfg<128, 128, 16, 8, 8>(a, vec, s);  // 256 threads
+    case 6: return launch_cfg<64, 32, 32, 4, 4>(a, vec, s);    // 128 threads
+    default: return launch_cfg<128, 64, 32, 8, 8>(a, vec, s);  // 128 threads
+    }
 }
 
 }  // namespace fg

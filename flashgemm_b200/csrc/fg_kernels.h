@@ -79,6 +79,20 @@ cudaError_t launch_prep_int8_weights(const int8_t *src, long ld_in, uint8_t *dst
                                      long M, long K, long tail_lo, long tail_hi,
                                      cudaStream_t s);
 
+// The same preparation for up to 8 matrices in one launch.
+struct PrepJob {
+    const int8_t *src;
+    long ld_in;
+    uint8_t *dst;
+    long ld_out;
+    long M, K, tail_lo, tail_hi;
+};
+struct PrepJobs {
+    PrepJob job[8];
+    int n;
+};
+cudaError_t launch_prep_int8_jobs(const PrepJobs &jobs, cudaStream_t s);
+
 // Fill `count` 32-bit words with `value`.
 cudaError_t launch_fill_u32(uint32_t *dst, size_t count, uint32_t value, cudaStream_t s);
 

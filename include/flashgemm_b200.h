@@ -59,6 +59,16 @@ int fg_get_f32_algo(void);
 void fg_set_sgemm_algo(int algo);
 int fg_get_sgemm_algo(void);
 
+/* How BF16 / INT8 chains are launched.
+ * FG_CHAIN_FUSED (default): the whole chain in one persistent launch; a stage
+ *   starts on a 256-column block as soon as the previous stage has stored it.
+ * FG_CHAIN_PER_GEMM: one tensor-core launch per GEMM, the plain per-GEMM path
+ *   (same kernels' arithmetic, so the same results).
+ * The environment variable FG_FUSED=0 selects the per-GEMM path initially. */
+enum { FG_CHAIN_FUSED = 0, FG_CHAIN_PER_GEMM = 1 };
+void fg_set_chain_mode(int mode);
+int fg_get_chain_mode(void);
+
 /* Element types of a chain. */
 enum { FG_DT_F32 = 0, FG_DT_BF16 = 1, FG_DT_INT8 = 2 };
 

@@ -278,3 +278,20 @@ def test_mismatched_chain_is_rejected(fg):
     C = np.zeros((32, 64), np.int32)
     fg.flashgemm_multi_int8uint8int32(C, B, 64, 2, As[0], 32, 64, As[1], 32, 48)
     assert fg.last_status() == fg.FG_ERR_INVALID
+
+
+@pytest.mark.parametrize("dt", ["int8", "bf16"])
+def test_fused_chain_equals_per_gemm_path(fg, dt):
+    """One persistent launch for the whole chain computes exactly what one
+    launch per GEMM computes (same tiles, same k order)."""
+    N, K1, Ms = 1280, 256, [384, 520, 136, 64]
+    B, As, Ks = oracle.chain_inputs(dt, N, K1, Ms, seed=31)
+    fg.set_chain_mode("per_gemm")
+    try:
+        a = run_chain(fg, dt, B, As, N, Ms, Ks)
+    finally:
+        fg.set_chain_mode("fused")
+    b = run_chain(fg, dt, B, As, N, Ms, Ks)
+    np.testing.assert_array_equal(a, b)
+    want = oracle.chain(dt, B, As, N, Ms, Ks, mode=oracle.REF, threads=1)
+    assert_parity(dt, b, want, (Ms[-1] // 4) * 4 if dt == "int8" else None)
