@@ -262,3 +262,60 @@ def shard_columns(N, world, rank, panel=32):
     p0 = rank * per + min(rank, extra)
     p1 = p0 + per + (1 if rank < extra else 0)
     return min(p0 * panel, N), min(p1 * panel, N)
+
+
+# ------------------------------------------------------------ weight registry
+
+FG_MEM_HOST, FG_MEM_DEVICE = 0, 1
+
+
+class Weights:
+    """A weight matrix registered on the current device (fg_weights_register):
+    copied once in the kernels' layout with its derived forms prepared once."""
+
+    def __init__(self, dtype, A, M=None, K=None):
+        L = lib()
+        L.fg_weights_register.argtypes = [ctypes.c_int, _P, _L, _L, ctypes.c_int,
+                                          ctypes.POINTER(_P)]
+        L.fg_weights_bytes.restype = _L
+        L.fg_weights_bytes.argtypes = [_P]
+        L.fg_weights_release.argtypes = [_P]
+        if isinstance(A, np.ndarray):
+            M, K = A.shape if M is None else (M, K)
+            ptr, where = A.ctypes.data_as(_P), FG_MEM_HOST
+        else:  # torch CUDA tensor
+            M, K = tuple(A.shape) if M is None else (M, K)
+            ptr, where = _P(A.data_ptr()), FG_MEM_DEVICE
+        h = _P()
+        st = L.fg_weights_register(_DT[dtype], ptr, int(M), int(K), where, ctypes.byref(h))
+        if st != FG_OK:
+            raise FlashgemmError(st, last_error())
+        self.handle, self.dtype, self.M, self.K = h, dtype, int(M), int(K)
+
+    @property
+    def nbytes(self):
+        return int(lib().fg_weights_bytes(self.handle))
+
+    def release(self):
+        if self.handle:
+            lib().fg_weights_release(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+
+def chain_registered(dtype, C, B, N, weights, stream=None):
+    """Chain on registered weights (list of Weights) with device B and C."""
+    import torch
+    L = lib()
+    L.fg_chain_registered.argtypes = [ctypes.c_int, _P, _P, _L, ctypes.c_int, _P, _P]
+    n = len(weights)
+    hs = (_P * n)(*[w.handle for w in weights])
+    s = (stream or torch.cuda.current_stream()).cuda_stream
+    st = L.fg_chain_registered(_DT[dtype], C.data_ptr(), B.data_ptr(), int(N), n, hs, s)
+    if st != FG_OK:
+        raise FlashgemmError(st, last_error())

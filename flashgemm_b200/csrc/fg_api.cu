@@ -383,11 +383,24 @@ int launch_stages(DevCtx *c, int kind, std::vector<StageArgs> &stages, long N)
     return FG_OK;
 }
 
+// Weights already laid out for the kernels (the weight registry keeps these):
+// w / ld: the A operand (BF16, INT8, or FP32 for the FFMA path); hi / lo:
+// the 3xTF32 split (FP32 only); tail: the INT8 reference tail block.
+struct PreparedW {
+    const void *w;
+    long ld;
+    const float *hi, *lo;
+    long ld_split;
+    const uint8_t *tail;
+    long ld_tail;
+    int tail_row0, tail_lo, tail_hi;
+};
+
 // Runs the chain on c->stream. Device operands: B (K[0] x N, ld b.ld),
 // A[i] (M[i] x K[i], ld a[i].ld, 16-byte-aligned rows where the tensor path
 // needs them), C (M[n-1] x N, ld ldc). Scratch must already be reserved.
 int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b, long N, int n,
-              const Mat *a, const long *M, const long *K)
+              const Mat *a, const long *M, const long *K, const PreparedW *pw = nullptr)
 {
     const long ldN = round_up(N, 16);
     const bool ref = (sem == FG_SEM_REF);
@@ -405,7 +418,8 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
         for (int i = 0; i < n; ++i) {
             FfmaArgs f;
             f.M = (int)M[i]; f.N = (int)N; f.K = (int)K[i];
-            f.A = (const float *)a[i].p; f.lda = a[i].ld;
+            f.A = pw ? (const float *)pw[i].w : (const float *)a[i].p;
+            f.lda = pw ? pw[i].ld : a[i].ld;
             f.B = x; f.ldb = ldx;
             const bool last = (i == n - 1);
             f.C = last ? (float *)C : buf[i & 1];
@@ -426,14 +440,24 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
     s.N = (int)N;
 
     if (dtype == FG_DT_F32) {  // 3xTF32
-        std::vector<float *> wh(n), wl(n);
+        std::vector<const float *> wh(n), wl(n);
+        std::vector<long> wld(n);
         for (int i = 0; i < n; ++i) {
             const long ldk = round_up(K[i], 4);
-            wh[i] = (float *)arena_take(c, (size_t)M[i] * ldk * 4);
-            wl[i] = (float *)arena_take(c, (size_t)M[i] * ldk * 4);
+            wld[i] = ldk;
+            if (pw) {
+                wh[i] = pw[i].hi;
+                wl[i] = pw[i].lo;
+                wld[i] = pw[i].ld_split;
+                continue;
+            }
+            float *h = (float *)arena_take(c, (size_t)M[i] * ldk * 4);
+            float *l = (float *)arena_take(c, (size_t)M[i] * ldk * 4);
+            wh[i] = h;
+            wl[i] = l;
             int st = run_kernel(c, FG_PK_AUX, 0.0, "tf32 split (weights)", [&] {
-                return launch_split_tf32((const float *)a[i].p, a[i].ld, wh[i], wl[i], ldk, M[i],
-                                         K[i], c->stream);
+                return launch_split_tf32((const float *)a[i].p, a[i].ld, h, l, ldk, M[i], K[i],
+                                         c->stream);
             });
             if (st) return st;
         }
@@ -453,7 +477,7 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             const bool last = (i == n - 1);
             s.op = OP_TF32X3;
             s.M = (int)M[i]; s.K = (int)K[i];
-            s.w = wh[i]; s.w_lo = wl[i]; s.ld_w = round_up(K[i], 4);
+            s.w = wh[i]; s.w_lo = wl[i]; s.ld_w = wld[i];
             s.x = xh; s.x_lo = xl; s.ld_x = ldN;
             s.epi = last ? EPI_F32 : EPI_TF32SPLIT;
             s.out = last ? C : (void *)ph[i & 1];
@@ -481,8 +505,8 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
         long ldx = b.ld;
         std::vector<StageArgs> stages;
         for (int i = 0; i < n; ++i) {
-            const void *w = a[i].p;
-            long ldw = a[i].ld;
+            const void *w = pw ? pw[i].w : a[i].p;
+            long ldw = pw ? pw[i].ld : a[i].ld;
             if ((ldw % 8) || ((uintptr_t)w % 16)) {
                 const long ldk = round_up(K[i], 8);
                 void *wp = arena_take(c, (size_t)M[i] * ldk * 2);
@@ -535,8 +559,8 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             // (TMA); otherwise through a padded copy. Tail rows always come from a
             // prepared copy of the 256-row block that holds them.
             const long ldw = round_up(Ki + 4, 16);
-            const void *wmain = a[i].p;
-            long ldmain = a[i].ld;
+            const void *wmain = pw ? pw[i].w : a[i].p;
+            long ldmain = pw ? pw[i].ld : a[i].ld;
             if ((ldmain % 16) || !aligned16(wmain)) {
                 uint8_t *wp = (uint8_t *)arena_take(c, (size_t)Mi * ldw);
                 int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 weight copy", [&] {
@@ -550,7 +574,11 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             s.w_tail = nullptr;
             s.ld_w_tail = 0;
             s.tail_row0 = 0;
-            if (tail_hi > tail_lo) {
+            if (tail_hi > tail_lo && pw && pw[i].tail) {  // prepared at registration
+                s.w_tail = pw[i].tail;
+                s.ld_w_tail = pw[i].ld_tail;
+                s.tail_row0 = pw[i].tail_row0;
+            } else if (tail_hi > tail_lo) {
                 const long row0 = (tail_lo / 256) * 256;
                 uint8_t *wt = (uint8_t *)arena_take(c, (size_t)(Mi - row0) * ldw);
                 if (jobs.n == 8) {  // flush a full batch
@@ -743,6 +771,138 @@ int fence_out(DevCtx *c, void *user)
     CUDA_TRY(cudaEventRecord(c->ev_out, c->stream));
     CUDA_TRY(cudaStreamWaitEvent((cudaStream_t)user, c->ev_out, 0));
     return FG_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- weight registry
+
+struct fg_weights_s {
+    int dtype;
+    int dev;
+    long M, K;
+    void *main = nullptr;  // A operand layout (BF16 ld % 8, INT8 ld % 16, FP32 ld % 4)
+    long ld = 0;
+    float *hi = nullptr, *lo = nullptr;  // FP32: 3xTF32 split
+    uint8_t *tail = nullptr;             // INT8: reference tail block
+    long ld_tail = 0;
+    int tail_row0 = 0, tail_lo = 0, tail_hi = 0;
+    size_t bytes = 0;
+};
+
+namespace {
+
+void free_weights(fg_weights_s *w)
+{
+    if (!w) return;
+    cudaFree(w->main);
+    cudaFree(w->hi);
+    cudaFree(w->lo);
+    cudaFree(w->tail);
+    delete w;
+}
+
+int register_weights(int dtype, const void *A, long M, long K, int where, fg_weights_s **out)
+{
+    if (dtype != FG_DT_F32 && dtype != FG_DT_BF16 && dtype != FG_DT_INT8)
+        return fail(FG_ERR_INVALID, "unknown dtype %d", dtype);
+    if (!A || !out) return fail(FG_ERR_INVALID, "null pointer");
+    if (M <= 0 || K <= 0 || M > (1l << 30) || K > (1l << 30))
+        return fail(FG_ERR_INVALID, "M and K must be positive");
+    if (where != FG_MEM_HOST && where != FG_MEM_DEVICE)
+        return fail(FG_ERR_INVALID, "where must be FG_MEM_HOST or FG_MEM_DEVICE");
+    DevCtx *c;
+    int st;
+    if ((st = get_ctx(&c))) return st;
+    std::lock_guard<std::mutex> lk(c->mu);
+    const int elt = elt_of(dtype);
+    fg_weights_s *w = new fg_weights_s;
+    w->dtype = dtype;
+    w->dev = c->dev;
+    w->M = M;
+    w->K = K;
+    w->ld = round_up(K, 16 / elt);
+    auto alloc = [&](void **p, size_t bytes) -> int {
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(FG_ERR_NOMEM, "weights: %zu bytes: %s", bytes, cudaGetErrorString(e));
+        }
+        w->bytes += bytes;
+        return FG_OK;
+    };
+    const size_t main_bytes = (size_t)M * w->ld * elt;
+    if ((st = alloc(&w->main, main_bytes))) {
+        free_weights(w);
+        return st;
+    }
+    cudaError_t e = cudaMemsetAsync(w->main, 0, main_bytes, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(w->main, w->ld * elt, A, K * elt, K * elt, M,
+                              where == FG_MEM_HOST ? cudaMemcpyHostToDevice
+                                                   : cudaMemcpyDeviceToDevice,
+                              c->stream);
+    if (e != cudaSuccess) {
+        free_weights(w);
+        return fail(FG_ERR_CUDA, "weights copy: %s", cudaGetErrorString(e));
+    }
+    if (dtype == FG_DT_F32) {
+        const size_t b = (size_t)M * w->ld * 4;
+        if ((st = alloc((void **)&w->hi, b)) || (st = alloc((void **)&w->lo, b))) {
+            free_weights(w);
+            return st;
+        }
+        if ((st = launch(launch_split_tf32((const float *)w->main, w->ld, w->hi, w->lo, w->ld, M,
+                                           K, c->stream),
+                         "tf32 split (registered weights)"))) {
+            free_weights(w);
+            return st;
+        }
+    }
+    if (dtype == FG_DT_INT8 && K % 4 == 0 && K >= 4 && (M / 4) * 4 > (M / 12) * 12) {
+        // the reference's shifted tail rows (multigemm/src/kernel_int8.h:771-1057)
+        w->tail_lo = (int)((M / 12) * 12);
+        w->tail_hi = (int)((M / 4) * 4);
+        w->tail_row0 = (w->tail_lo / 256) * 256;
+        w->ld_tail = round_up(K + 4, 16);
+        const long rows = M - w->tail_row0;
+        if ((st = alloc((void **)&w->tail, (size_t)rows * w->ld_tail))) {
+            free_weights(w);
+            return st;
+        }
+        if ((st = launch(launch_prep_int8_weights((const int8_t *)w->main + (size_t)w->tail_row0 * w->ld,
+                                                  w->ld, w->tail, w->ld_tail, rows, K,
+                                                  w->tail_lo - w->tail_row0,
+                                                  w->tail_hi - w->tail_row0, c->stream),
+                         "int8 tail-row prep (registered weights)"))) {
+            free_weights(w);
+            return st;
+        }
+    }
+    e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        free_weights(w);
+        return fail(FG_ERR_CUDA, "weights: %s", cudaGetErrorString(e));
+    }
+    *out = w;
+    return ok();
+}
+
+PreparedW prepared_of(const fg_weights_s *w)
+{
+    PreparedW p;
+    memset(&p, 0, sizeof p);
+    p.w = w->main;
+    p.ld = w->ld;
+    p.hi = w->hi;
+    p.lo = w->lo;
+    p.ld_split = w->ld;
+    p.tail = w->tail;
+    p.ld_tail = w->ld_tail;
+    p.tail_row0 = w->tail_row0;
+    p.tail_lo = w->tail_lo;
+    p.tail_hi = w->tail_hi;
+    return p;
 }
 
 }  // namespace
@@ -974,5 +1134,77 @@ FG_EXPORT int fg_profile_query(int kind, double *total_ms, unsigned long long *l
     if (total_ms) *total_ms = ms;
     if (launches) *launches = n;
     if (flops) *flops = fl;
+    return ok();
+}
+
+FG_EXPORT int fg_weights_register(int dtype, const void *A, long M, long K, int where,
+                                  fg_weights *out)
+{
+    return register_weights(dtype, A, M, K, where, out);
+}
+
+FG_EXPORT int fg_weights_release(fg_weights w)
+{
+    if (!w) return ok();
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != w->dev) cudaSetDevice(w->dev);
+    cudaDeviceSynchronize();  // no chain may still read them
+    free_weights(w);
+    if (cur != w->dev) cudaSetDevice(cur);
+    return ok();
+}
+
+FG_EXPORT long fg_weights_bytes(fg_weights w) { return w ? (long)w->bytes : 0; }
+
+FG_EXPORT int fg_chain_registered(int dtype, void *C, const void *B, long N, int num_gemm,
+                                  const fg_weights *W, void *stream)
+{
+    if (!C || !B || !W) return fail(FG_ERR_INVALID, "null pointer");
+    if (num_gemm < 1 || num_gemm > 4096) return fail(FG_ERR_INVALID, "num_gemm out of range");
+    std::vector<long> M(num_gemm), K(num_gemm);
+    std::vector<PreparedW> pw(num_gemm);
+    std::vector<Mat> a(num_gemm);
+    for (int i = 0; i < num_gemm; ++i) {
+        if (!W[i]) return fail(FG_ERR_INVALID, "null weight handle");
+        if (W[i]->dtype != dtype) return fail(FG_ERR_INVALID, "gemm %d: weights of another dtype", i + 1);
+        M[i] = W[i]->M;
+        K[i] = W[i]->K;
+        pw[i] = prepared_of(W[i]);
+        a[i] = Mat{W[i]->main, W[i]->ld};
+    }
+    int st = check_shapes(dtype, N, num_gemm, M.data(), K.data());
+    if (st) return st;
+    for (int i = 0; i < num_gemm; ++i)
+        if (K[i] % 2 != 0) return fail(FG_ERR_INVALID, "gemm %d: K must be a multiple of 2", i + 1);
+    if (N == 0) return ok();
+    if (!aligned16(C) || !aligned16(B))
+        return fail(FG_ERR_INVALID, "device pointers must be 16-byte aligned");
+    DevCtx *c;
+    if ((st = get_ctx(&c))) return st;
+    for (int i = 0; i < num_gemm; ++i)
+        if (W[i]->dev != c->dev)
+            return fail(FG_ERR_INVALID, "gemm %d: weights registered on device %d", i + 1, W[i]->dev);
+    std::lock_guard<std::mutex> lk(c->mu);
+    const int elt = elt_of(dtype);
+    const int algo = f32_algo();
+    const long ldN = round_up(N, 16);
+    const bool tensor = !(dtype == FG_DT_F32 && algo == FG_F32_FFMA);
+    const bool pad_b = tensor && ((N * elt) % 16 != 0);
+    size_t need = chain_scratch(dtype, algo, N, num_gemm, M.data(), K.data()) + 4096;
+    if (pad_b) need += carve_size((size_t)K[0] * ldN * elt);
+    if ((st = arena_reserve(c, need))) return st;
+    if ((st = fence_in(c, stream))) return st;
+    Mat b{B, N};
+    if (pad_b) {
+        void *p = arena_take(c, (size_t)K[0] * ldN * elt);
+        CUDA_TRY(cudaMemcpy2DAsync(p, ldN * elt, B, N * elt, N * elt, K[0], cudaMemcpyDeviceToDevice,
+                                   c->stream));
+        b = Mat{p, ldN};
+    }
+    if ((st = run_chain(c, dtype, semantics(), algo, C, N, b, N, num_gemm, a.data(), M.data(),
+                        K.data(), pw.data())))
+        return st;
+    if ((st = fence_out(c, stream))) return st;
     return ok();
 }

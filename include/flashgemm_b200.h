@@ -89,6 +89,25 @@ int fg_chain_dev(int dtype, void *C, const void *B, long N, int num_gemm, const 
 int fg_sgemm_dev(float *C, const float *A, const float *B, long M, long N, long K, int algo,
                  void *stream);
 
+/* Weight registry: weights copied once to the current device in the layout
+ * the kernels read (16-byte rows), with their derived forms prepared once
+ * (FP32: the 3xTF32 hi/lo split; INT8: the reference's shifted tail-row
+ * block), so chains on them skip every per-call weight preparation. A is
+ * M x K row-major (leading dimension K) in host (FG_MEM_HOST) or device
+ * (FG_MEM_DEVICE) memory. Blocking. */
+typedef struct fg_weights_s *fg_weights;
+enum { FG_MEM_HOST = 0, FG_MEM_DEVICE = 1 };
+int fg_weights_register(int dtype, const void *A, long M, long K, int where, fg_weights *out);
+/* Device bytes a registered weight set holds. */
+long fg_weights_bytes(fg_weights w);
+/* Waits for the device to be idle, then frees the weights. */
+int fg_weights_release(fg_weights w);
+
+/* Chain on registered weights (W[i] gives M_i, K_i; K_{i+1} must equal M_i):
+ * device B (K_0 x N) and C (M_{n-1} x N), like fg_chain_dev. */
+int fg_chain_registered(int dtype, void *C, const void *B, long N, int num_gemm,
+                        const fg_weights *W, void *stream);
+
 /* Wait for all of the library's work on the current device and report any
  * kernel-side error since the last fg_sync (then cleared). */
 int fg_sync(void);

@@ -295,3 +295,35 @@ def test_fused_chain_equals_per_gemm_path(fg, dt):
     np.testing.assert_array_equal(a, b)
     want = oracle.chain(dt, B, As, N, Ms, Ks, mode=oracle.REF, threads=1)
     assert_parity(dt, b, want, (Ms[-1] // 4) * 4 if dt == "int8" else None)
+
+
+@pytest.mark.parametrize("dt,f32algo", [("int8", None), ("bf16", None), ("f32", "ffma"),
+                                        ("f32", "3xtf32")])
+def test_registered_weights_match_per_call_weights(fg, dt, f32algo):
+    """Weights registered once (copied, TF32-split / INT8 tail rows prepared)
+    give exactly the per-call entry point's results, call after call."""
+    import torch
+    N, K1, Ms = 768, 200, [268, 1000, 44]   # INT8 tail rows in every stage, one past row 256
+    if dt == "f32":
+        fg.set_f32_algo(f32algo)
+    try:
+        B, As, Ks = oracle.chain_inputs(dt, N, K1, Ms, seed=41)
+        if dt == "int8":
+            K1, Ks = 256, [256] + Ms[:-1]
+            B, As, _ = oracle.chain_inputs(dt, N, K1, Ms, seed=41)
+        host = run_chain(fg, dt, B, As, N, Ms, Ks)
+        W = [fg.Weights(dt, a) for a in As]
+        assert all(w.nbytes > 0 for w in W)
+        tB = torch.from_numpy(B.view(np.int8) if dt == "int8" else
+                              (B.view(np.int16) if dt == "bf16" else B)).cuda()
+        for _ in range(2):
+            tC = torch.zeros((Ms[-1], N), dtype=torch.int32 if dt == "int8" else torch.float32,
+                             device="cuda")
+            fg.chain_registered(dt, tC, tB, N, W)
+            torch.cuda.synchronize()
+            fg.sync()
+            np.testing.assert_array_equal(tC.cpu().numpy(), host)
+        for w in W:
+            w.release()
+    finally:
+        fg.set_f32_algo("3xtf32")
