@@ -319,3 +319,26 @@ def chain_registered(dtype, C, B, N, weights, stream=None):
     st = L.fg_chain_registered(_DT[dtype], C.data_ptr(), B.data_ptr(), int(N), n, hs, s)
     if st != FG_OK:
         raise FlashgemmError(st, last_error())
+
+
+class _ChainDesc(ctypes.Structure):
+    _fields_ = [("C", _P), ("B", _P), ("N", _L), ("num_gemm", ctypes.c_int), ("W", _P)]
+
+
+def chain_group(dtype, chains, stream=None):
+    """Many chains in one persistent launch. chains: list of (C, B, N, [Weights])
+    with torch CUDA tensors for C and B."""
+    import torch
+    L = lib()
+    L.fg_chain_group.argtypes = [ctypes.c_int, ctypes.c_int, _P, _P]
+    keep = []
+    descs = (_ChainDesc * len(chains))()
+    for d, (C, B, N, W) in zip(descs, chains):
+        hs = (_P * len(W))(*[w.handle for w in W])
+        keep.append(hs)
+        d.C, d.B, d.N, d.num_gemm = C.data_ptr(), B.data_ptr(), int(N), len(W)
+        d.W = ctypes.cast(hs, _P)
+    s = (stream or torch.cuda.current_stream()).cuda_stream
+    st = L.fg_chain_group(_DT[dtype], len(chains), ctypes.cast(descs, _P), s)
+    if st != FG_OK:
+        raise FlashgemmError(st, last_error())

@@ -351,8 +351,8 @@ int launch_stages(DevCtx *c, int kind, std::vector<StageArgs> &stages, long N)
             char path[1024];
             snprintf(path, sizeof path, "%s/chain_trace_%d.csv", trace_dir, seq++);
             if (FILE *f = fopen(path, "w")) {
-                fprintf(f, "item,cta,sm,prod_start,dep_done,prod_end,mma_start,mma_end,epi_start,"
-                           "epi_issued,epi_end\n");
+                fprintf(f, "q,cta,entry,sm,prod_start,dep_done,prod_end,mma_start,mma_end,"
+                           "epi_start,epi_issued,epi_end\n");
                 const int nf = chain_trace_fields();
                 for (size_t r = 0; r < trace_words / nf; ++r) {
                     fprintf(f, "%zu,%zu", r / 2, r % 2);
@@ -395,6 +395,146 @@ struct PreparedW {
     long ld_tail;
     int tail_row0, tail_lo, tail_hi;
 };
+
+// Builds the stage list of a BF16 or INT8 chain (between-stage buffers from the
+// arena, weight preparations launched on c->stream) without launching the stages.
+int build_tc_stages(DevCtx *c, int dtype, int sem, void *C, long ldc, Mat b, long N, int n,
+                    const Mat *a, const long *M, const long *K, const PreparedW *pw,
+                    std::vector<StageArgs> &out)
+{
+    const long ldN = round_up(N, 16);
+    const bool ref = (sem == FG_SEM_REF);
+    long maxM = 0;
+    for (int i = 0; i < n - 1; ++i) maxM = M[i] > maxM ? M[i] : maxM;
+    StageArgs s;
+    memset(&s, 0, sizeof s);
+    s.status = c->status;
+    s.N = (int)N;
+    if (dtype == FG_DT_BF16) {
+        uint16_t *buf[2] = {nullptr, nullptr};
+        if (n > 1) {
+            buf[0] = (uint16_t *)arena_take(c, (size_t)maxM * ldN * 2);
+            buf[1] = (uint16_t *)arena_take(c, (size_t)maxM * ldN * 2);
+        }
+        const void *x = b.p;
+        long ldx = b.ld;
+        std::vector<StageArgs> stages;
+        for (int i = 0; i < n; ++i) {
+            const void *w = pw ? pw[i].w : a[i].p;
+            long ldw = pw ? pw[i].ld : a[i].ld;
+            if ((ldw % 8) || ((uintptr_t)w % 16)) {
+                const long ldk = round_up(K[i], 8);
+                void *wp = arena_take(c, (size_t)M[i] * ldk * 2);
+                CUDA_TRY(cudaMemsetAsync(wp, 0, (size_t)M[i] * ldk * 2, c->stream));
+                CUDA_TRY(cudaMemcpy2DAsync(wp, ldk * 2, w, ldw * 2, K[i] * 2, M[i],
+                                           cudaMemcpyDeviceToDevice, c->stream));
+                w = wp;
+                ldw = ldk;
+            }
+            const bool last = (i == n - 1);
+            s.op = OP_BF16;
+            s.M = (int)M[i]; s.K = (int)K[i];
+            s.w = w; s.ld_w = ldw;
+            s.x = x; s.ld_x = ldx;
+            s.epi = last ? EPI_F32 : EPI_BF16;
+            s.out = last ? C : (void *)buf[i & 1];
+            s.ld_out = last ? ldc : ldN;
+            s.permute = ref ? 1 : 0;
+            s.m_written = (int)M[i];
+            s.tail_lo = s.tail_hi = 0;
+            stages.push_back(s);
+            x = s.out;
+            ldx = s.ld_out;
+        }
+        out = std::move(stages);
+        return FG_OK;
+    }
+
+    // INT8
+    {
+        uint8_t *buf[2] = {nullptr, nullptr};
+        if (n > 1) {
+            buf[0] = (uint8_t *)arena_take(c, (size_t)maxM * ldN);
+            buf[1] = (uint8_t *)arena_take(c, (size_t)maxM * ldN);
+        }
+        const void *x = b.p;
+        long ldx = b.ld;
+        std::vector<StageArgs> stages;
+        PrepJobs jobs;
+        jobs.n = 0;
+        for (int i = 0; i < n; ++i) {
+            const long Mi = M[i], Ki = K[i];
+            // reference tail rows (multigemm/src/kernel_int8.h:771-1057): only with
+            // whole k-quads; other K leave the reference undefined and get no shift
+            long tail_lo = 0, tail_hi = 0;
+            if (ref && Ki % 4 == 0 && Ki >= 4) {
+                tail_lo = (Mi / 12) * 12;
+                tail_hi = (Mi / 4) * 4;
+            }
+            // Weights go to the MMA as they are when their rows are 16-byte aligned
+            // (TMA); otherwise through a padded copy. Tail rows always come from a
+            // prepared copy of the 256-row block that holds them.
+            const long ldw = round_up(Ki + 4, 16);
+            const void *wmain = pw ? pw[i].w : a[i].p;
+            long ldmain = pw ? pw[i].ld : a[i].ld;
+            if ((ldmain % 16) || !aligned16(wmain)) {
+                uint8_t *wp = (uint8_t *)arena_take(c, (size_t)Mi * ldw);
+                int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 weight copy", [&] {
+                    return launch_prep_int8_weights((const int8_t *)a[i].p, a[i].ld, wp, ldw, Mi,
+                                                    Ki, 0, 0, c->stream);
+                });
+                if (st) return st;
+                wmain = wp;
+                ldmain = ldw;
+            }
+            s.w_tail = nullptr;
+            s.ld_w_tail = 0;
+            s.tail_row0 = 0;
+            if (tail_hi > tail_lo && pw && pw[i].tail) {  // prepared at registration
+                s.w_tail = pw[i].tail;
+                s.ld_w_tail = pw[i].ld_tail;
+                s.tail_row0 = pw[i].tail_row0;
+            } else if (tail_hi > tail_lo) {
+                const long row0 = (tail_lo / 256) * 256;
+                uint8_t *wt = (uint8_t *)arena_take(c, (size_t)(Mi - row0) * ldw);
+                if (jobs.n == 8) {  // flush a full batch
+                    int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 tail-row prep",
+                                        [&] { return launch_prep_int8_jobs(jobs, c->stream); });
+                    if (st) return st;
+                    jobs.n = 0;
+                }
+                jobs.job[jobs.n++] = PrepJob{(const int8_t *)a[i].p + row0 * a[i].ld, a[i].ld, wt, ldw,
+                                             Mi - row0, Ki, tail_lo - row0, tail_hi - row0};
+                s.w_tail = wt;
+                s.ld_w_tail = ldw;
+                s.tail_row0 = (int)row0;
+            }
+            const bool last = (i == n - 1);
+            s.op = OP_I8;
+            s.M = (int)Mi; s.K = (int)Ki;
+            s.w = wmain; s.ld_w = ldmain;
+            s.x = x; s.ld_x = ldx;
+            s.epi = last ? EPI_S32 : EPI_S8;
+            s.out = last ? C : (void *)buf[i & 1];
+            s.ld_out = last ? ldc : ldN;
+            s.permute = ref ? 1 : 0;
+            s.m_written = (last && ref) ? (int)((Mi / 4) * 4) : (int)Mi;
+            s.tail_lo = (int)tail_lo;
+            s.tail_hi = (int)tail_hi;
+            stages.push_back(s);
+            x = s.out;
+            ldx = s.ld_out;
+        }
+        if (jobs.n) {  // all tail blocks of the chain in one launch
+            int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 tail-row prep",
+                                [&] { return launch_prep_int8_jobs(jobs, c->stream); });
+            if (st) return st;
+        }
+        out = std::move(stages);
+        return FG_OK;
+    }
+    return fail(FG_ERR_INVALID, "not a tensor-core chain dtype");
+}
 
 // Runs the chain on c->stream. Device operands: B (K[0] x N, ld b.ld),
 // A[i] (M[i] x K[i], ld a[i].ld, 16-byte-aligned rows where the tensor path
@@ -495,126 +635,11 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
         return FG_OK;
     }
 
-    if (dtype == FG_DT_BF16) {
-        uint16_t *buf[2] = {nullptr, nullptr};
-        if (n > 1) {
-            buf[0] = (uint16_t *)arena_take(c, (size_t)maxM * ldN * 2);
-            buf[1] = (uint16_t *)arena_take(c, (size_t)maxM * ldN * 2);
-        }
-        const void *x = b.p;
-        long ldx = b.ld;
-        std::vector<StageArgs> stages;
-        for (int i = 0; i < n; ++i) {
-            const void *w = pw ? pw[i].w : a[i].p;
-            long ldw = pw ? pw[i].ld : a[i].ld;
-            if ((ldw % 8) || ((uintptr_t)w % 16)) {
-                const long ldk = round_up(K[i], 8);
-                void *wp = arena_take(c, (size_t)M[i] * ldk * 2);
-                CUDA_TRY(cudaMemsetAsync(wp, 0, (size_t)M[i] * ldk * 2, c->stream));
-                CUDA_TRY(cudaMemcpy2DAsync(wp, ldk * 2, w, ldw * 2, K[i] * 2, M[i],
-                                           cudaMemcpyDeviceToDevice, c->stream));
-                w = wp;
-                ldw = ldk;
-            }
-            const bool last = (i == n - 1);
-            s.op = OP_BF16;
-            s.M = (int)M[i]; s.K = (int)K[i];
-            s.w = w; s.ld_w = ldw;
-            s.x = x; s.ld_x = ldx;
-            s.epi = last ? EPI_F32 : EPI_BF16;
-            s.out = last ? C : (void *)buf[i & 1];
-            s.ld_out = last ? ldc : ldN;
-            s.permute = ref ? 1 : 0;
-            s.m_written = (int)M[i];
-            s.tail_lo = s.tail_hi = 0;
-            stages.push_back(s);
-            x = s.out;
-            ldx = s.ld_out;
-        }
-        return launch_stages(c, FG_PK_TC_BF16, stages, N);
-    }
-
-    // INT8
     {
-        uint8_t *buf[2] = {nullptr, nullptr};
-        if (n > 1) {
-            buf[0] = (uint8_t *)arena_take(c, (size_t)maxM * ldN);
-            buf[1] = (uint8_t *)arena_take(c, (size_t)maxM * ldN);
-        }
-        const void *x = b.p;
-        long ldx = b.ld;
         std::vector<StageArgs> stages;
-        PrepJobs jobs;
-        jobs.n = 0;
-        for (int i = 0; i < n; ++i) {
-            const long Mi = M[i], Ki = K[i];
-            // reference tail rows (multigemm/src/kernel_int8.h:771-1057): only with
-            // whole k-quads; other K leave the reference undefined and get no shift
-            long tail_lo = 0, tail_hi = 0;
-            if (ref && Ki % 4 == 0 && Ki >= 4) {
-                tail_lo = (Mi / 12) * 12;
-                tail_hi = (Mi / 4) * 4;
-            }
-            // Weights go to the MMA as they are when their rows are 16-byte aligned
-            // (TMA); otherwise through a padded copy. Tail rows always come from a
-            // prepared copy of the 256-row block that holds them.
-            const long ldw = round_up(Ki + 4, 16);
-            const void *wmain = pw ? pw[i].w : a[i].p;
-            long ldmain = pw ? pw[i].ld : a[i].ld;
-            if ((ldmain % 16) || !aligned16(wmain)) {
-                uint8_t *wp = (uint8_t *)arena_take(c, (size_t)Mi * ldw);
-                int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 weight copy", [&] {
-                    return launch_prep_int8_weights((const int8_t *)a[i].p, a[i].ld, wp, ldw, Mi,
-                                                    Ki, 0, 0, c->stream);
-                });
-                if (st) return st;
-                wmain = wp;
-                ldmain = ldw;
-            }
-            s.w_tail = nullptr;
-            s.ld_w_tail = 0;
-            s.tail_row0 = 0;
-            if (tail_hi > tail_lo && pw && pw[i].tail) {  // prepared at registration
-                s.w_tail = pw[i].tail;
-                s.ld_w_tail = pw[i].ld_tail;
-                s.tail_row0 = pw[i].tail_row0;
-            } else if (tail_hi > tail_lo) {
-                const long row0 = (tail_lo / 256) * 256;
-                uint8_t *wt = (uint8_t *)arena_take(c, (size_t)(Mi - row0) * ldw);
-                if (jobs.n == 8) {  // flush a full batch
-                    int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 tail-row prep",
-                                        [&] { return launch_prep_int8_jobs(jobs, c->stream); });
-                    if (st) return st;
-                    jobs.n = 0;
-                }
-                jobs.job[jobs.n++] = PrepJob{(const int8_t *)a[i].p + row0 * a[i].ld, a[i].ld, wt, ldw,
-                                             Mi - row0, Ki, tail_lo - row0, tail_hi - row0};
-                s.w_tail = wt;
-                s.ld_w_tail = ldw;
-                s.tail_row0 = (int)row0;
-            }
-            const bool last = (i == n - 1);
-            s.op = OP_I8;
-            s.M = (int)Mi; s.K = (int)Ki;
-            s.w = wmain; s.ld_w = ldmain;
-            s.x = x; s.ld_x = ldx;
-            s.epi = last ? EPI_S32 : EPI_S8;
-            s.out = last ? C : (void *)buf[i & 1];
-            s.ld_out = last ? ldc : ldN;
-            s.permute = ref ? 1 : 0;
-            s.m_written = (last && ref) ? (int)((Mi / 4) * 4) : (int)Mi;
-            s.tail_lo = (int)tail_lo;
-            s.tail_hi = (int)tail_hi;
-            stages.push_back(s);
-            x = s.out;
-            ldx = s.ld_out;
-        }
-        if (jobs.n) {  // all tail blocks of the chain in one launch
-            int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 tail-row prep",
-                                [&] { return launch_prep_int8_jobs(jobs, c->stream); });
-            if (st) return st;
-        }
-        return launch_stages(c, FG_PK_TC_I8, stages, N);
+        int st = build_tc_stages(c, dtype, sem, C, ldc, b, N, n, a, M, K, pw, stages);
+        if (st) return st;
+        return launch_stages(c, dtype == FG_DT_BF16 ? FG_PK_TC_BF16 : FG_PK_TC_I8, stages, N);
     }
 }
 
@@ -1205,6 +1230,104 @@ FG_EXPORT int fg_chain_registered(int dtype, void *C, const void *B, long N, int
     if ((st = run_chain(c, dtype, semantics(), algo, C, N, b, N, num_gemm, a.data(), M.data(),
                         K.data(), pw.data())))
         return st;
+    if ((st = fence_out(c, stream))) return st;
+    return ok();
+}
+
+// Many chains of one dtype on registered weights in one persistent launch.
+FG_EXPORT int fg_chain_group(int dtype, int nchains, const fg_chain_desc *chains, void *stream)
+{
+    if (nchains < 1 || !chains) return fail(FG_ERR_INVALID, "no chains");
+    if (dtype != FG_DT_BF16 && dtype != FG_DT_INT8 && dtype != FG_DT_F32)
+        return fail(FG_ERR_INVALID, "unknown dtype %d", dtype);
+    const int elt = elt_of(dtype);
+    long total_stages = 0;
+    for (int j = 0; j < nchains; ++j) {
+        const fg_chain_desc &d = chains[j];
+        if (!d.C || !d.B || !d.W || d.num_gemm < 1)
+            return fail(FG_ERR_INVALID, "chain %d: null pointer or no GEMM", j);
+        if (d.N <= 0 || (d.N * elt) % 16)
+            return fail(FG_ERR_INVALID, "chain %d: N must be positive with 16-byte rows", j);
+        if (!aligned16(d.C) || !aligned16(d.B))
+            return fail(FG_ERR_INVALID, "chain %d: pointers must be 16-byte aligned", j);
+        for (int i = 0; i < d.num_gemm; ++i) {
+            if (!d.W[i] || d.W[i]->dtype != dtype)
+                return fail(FG_ERR_INVALID, "chain %d gemm %d: weights missing or of another dtype",
+                            j, i + 1);
+            if (i > 0 && d.W[i]->K != d.W[i - 1]->M)
+                return fail(FG_ERR_INVALID, "chain %d gemm %d: K must equal the previous M", j,
+                            i + 1);
+            if (d.W[i]->K % 2) return fail(FG_ERR_INVALID, "chain %d: K must be even", j);
+        }
+        total_stages += d.num_gemm;
+    }
+    if (dtype == FG_DT_F32) {  // no grouped FP32 kernel: the chains run one after another
+        for (int j = 0; j < nchains; ++j) {
+            int st = fg_chain_registered(dtype, chains[j].C, chains[j].B, chains[j].N,
+                                         chains[j].num_gemm, chains[j].W, stream);
+            if (st) return st;
+        }
+        return ok();
+    }
+    DevCtx *c;
+    int st;
+    if ((st = get_ctx(&c))) return st;
+    std::lock_guard<std::mutex> lk(c->mu);
+    // scratch: every chain's between-stage buffers, counters and the tables
+    size_t need = 8192;
+    long work = 0, blocks = 0;
+    for (int j = 0; j < nchains; ++j) {
+        const fg_chain_desc &d = chains[j];
+        std::vector<long> M(d.num_gemm), K(d.num_gemm);
+        for (int i = 0; i < d.num_gemm; ++i) {
+            M[i] = d.W[i]->M;
+            K[i] = d.W[i]->K;
+            work += ((M[i] + 255) / 256) * ((d.N + 255) / 256);
+            blocks += (d.N + 255) / 256;
+        }
+        need += chain_scratch(dtype, 0, d.N, d.num_gemm, M.data(), K.data());
+    }
+    need += carve_size((size_t)blocks * sizeof(int)) +
+            carve_size(chain_group_table_bytes((int)total_stages, work));
+    if ((st = arena_reserve(c, need))) return st;
+    if ((st = fence_in(c, stream))) return st;
+    std::vector<StageArgs> all;
+    std::vector<int> prev;
+    for (int j = 0; j < nchains; ++j) {
+        const fg_chain_desc &d = chains[j];
+        const int n = d.num_gemm;
+        std::vector<long> M(n), K(n);
+        std::vector<PreparedW> pw(n);
+        std::vector<Mat> a(n);
+        for (int i = 0; i < n; ++i) {
+            M[i] = d.W[i]->M;
+            K[i] = d.W[i]->K;
+            pw[i] = prepared_of(d.W[i]);
+            a[i] = Mat{d.W[i]->main, d.W[i]->ld};
+        }
+        std::vector<StageArgs> stg;
+        if ((st = build_tc_stages(c, dtype, semantics(), d.C, d.N, Mat{d.B, d.N}, d.N, n, a.data(),
+                                  M.data(), K.data(), pw.data(), stg)))
+            return st;
+        const int base = (int)all.size();
+        for (int i = 0; i < n; ++i) {
+            all.push_back(stg[i]);
+            prev.push_back(i == 0 ? -1 : base + i - 1);
+        }
+    }
+    int *done = (int *)arena_take(c, (size_t)blocks * sizeof(int));
+    CUDA_TRY(cudaMemsetAsync(done, 0, (size_t)blocks * sizeof(int), c->stream));
+    void *tables = arena_take(c, chain_group_table_bytes((int)all.size(), work));
+    double fl = 0.0;
+    for (auto &x : all) fl += gemm_flops(x.M, x.N, x.K);
+    const int kind = dtype == FG_DT_BF16 ? FG_PK_TC_BF16 : FG_PK_TC_I8;
+    cudaError_t le = cudaSuccess;
+    st = run_kernel(c, kind, fl, "grouped chains", [&] {
+        le = launch_tc_group(all.data(), prev.data(), (int)all.size(), done, c->status, nullptr,
+                             tables, c->sms, c->stream);
+        return le;
+    });
+    if (st) return st;
     if ((st = fence_out(c, stream))) return st;
     return ok();
 }

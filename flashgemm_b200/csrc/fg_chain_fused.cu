@@ -21,6 +21,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -30,9 +31,9 @@
 
 namespace fg {
 
-constexpr int kChainMaxStages = 8;
+constexpr int kChainMaxStages = 8;      // stage table carried in the kernel parameters
 constexpr int kChainMaxPairs = 128;
-constexpr int kChainMaxItems = 10240;  // schedule entries carried in the kernel parameters
+constexpr int kParamSchedItems = 5632;  // work entries carried in the kernel parameters
 
 struct alignas(64) ChainStage {
     CUtensorMap tm_w;  // weights, M x K (box 128 rows x 128 bytes)
@@ -41,26 +42,36 @@ struct alignas(64) ChainStage {
     CUtensorMap tm_out;// stage output, for the staged (TMA-store) epilogue
     StageArgs a;       // shapes and epilogue of this stage
     int tiles_m;       // pair tiles (256 rows) along M
-    int item0;         // first work item of this stage
+    int tiles_n;       // 256-column blocks along N
+    int prev;          // stage whose output this stage reads (-1: first stage of its chain)
+    int done_off;      // this stage's column-block counters in `done`
 };
 
-// Work items are numbered stage by stage, column block by column block, row
-// block by row block; every dependency of an item has a smaller number. The
-// host assigns items to pairs (sched_off / sched: pair p runs items
-// sched[sched_off[p] .. sched_off[p+1]) in increasing order), so the smallest
-// unfinished item always heads its pair's list and the grid cannot deadlock.
+// Work entry: stage << 23 | row block << 12 | column block.
+__host__ __device__ constexpr uint32_t pack_item(int stage, int mb, int nb)
+{
+    return ((uint32_t)stage << 23) | ((uint32_t)mb << 12) | (uint32_t)nb;
+}
+
+// Work entries are ordered so that every dependency of an entry comes earlier
+// (a chain's stages in order); the host assigns entries to pairs (pair p runs
+// sched[off[p] .. off[p+1]) in that order), so the earliest unfinished entry
+// always heads its pair's list and the grid cannot deadlock. One chain's
+// tables fit in the parameters; a grouped launch of many chains passes them
+// in device memory (ext_*).
 struct ChainParams {
     ChainStage st[kChainMaxStages];
-    int nstages;
-    int tiles_n;      // 256-column blocks
-    int total_items;
+    const ChainStage *ext_st;
+    const uint32_t *ext_sched;
+    const int *ext_off;
     int npairs;
-    int *done;        // [nstages][tiles_n]: epilogue warps that finished a tile of the block
+    int *done;        // per (stage, column block): epilogue warps that finished a tile
     int *status;
-    unsigned long long *trace;  // optional: kTraceFields %globaltimer stamps per (item, CTA)
-    uint16_t sched_off[kChainMaxPairs + 1];
-    uint16_t sched[kChainMaxItems];
+    unsigned long long *trace;  // optional: kTraceFields stamps per (work entry, CTA)
+    int sched_off[kChainMaxPairs + 1];
+    uint32_t sched[kParamSchedItems];
 };
+static_assert(sizeof(ChainParams) <= 32000, "kernel parameter space");
 
 __device__ __forceinline__ int ld_acquire_gpu(const int *p)
 {
@@ -80,19 +91,9 @@ __device__ __forceinline__ void fence_proxy_async_global()
     asm volatile("fence.proxy.async.global;" ::: "memory");
 }
 
-__device__ __forceinline__ void decode_item(const ChainParams &P, int t, int &stage, int &mb,
-                                            int &nb)
-{
-    stage = 0;
-    while (stage + 1 < P.nstages && t >= P.st[stage + 1].item0) ++stage;
-    const int u = t - P.st[stage].item0;
-    nb = u / P.st[stage].tiles_m;
-    mb = u - nb * P.st[stage].tiles_m;
-}
-
 // Trace record of one (item, CTA): where the time of a fused chain goes.
-enum { TR_SM = 0, TR_PROD_START, TR_DEP_DONE, TR_PROD_END, TR_MMA_START, TR_MMA_END, TR_EPI_START,
-       TR_EPI_ISSUED, TR_EPI_END, kTraceFields };
+enum { TR_ENTRY = 0, TR_SM, TR_PROD_START, TR_DEP_DONE, TR_PROD_END, TR_MMA_START, TR_MMA_END,
+       TR_EPI_START, TR_EPI_ISSUED, TR_EPI_END, kTraceFields };
 
 __device__ __forceinline__ void trace_put(const ChainParams &P, int t, uint32_t rank, int f,
                                           unsigned long long v)
@@ -110,7 +111,29 @@ __device__ __forceinline__ uint32_t smid()
 // Epilogue warps per CTA (4) x CTAs per pair (2): counter increments per tile.
 constexpr int kDoneIncrementsPerTile = 8;
 
-template <int OP>
+// Stage i and work entry q, from the parameters (read through the constant
+// cache) or from device memory.
+template <bool EXT>
+__device__ __forceinline__ const ChainStage &stage_at(const ChainParams &P, int i)
+{
+    if constexpr (EXT)
+        return P.ext_st[i];
+    else
+        return P.st[i];
+}
+
+template <bool EXT>
+__device__ __forceinline__ uint32_t entry_at(const ChainParams &P, int q)
+{
+    if constexpr (EXT)
+        return P.ext_sched[q];
+    else
+        return P.sched[q];
+}
+
+// EXT: stage table and schedule in device memory (grouped launches) rather
+// than in the parameters (single chains, read through the constant cache).
+template <int OP, bool EXT>
 __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_constant__ ChainParams P)
 {
     using T = OpTraits<OP>;
@@ -129,6 +152,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
     const bool leader = (rank == 0);
     const int pair = blockIdx.x >> 1;
     int *status = P.status;
+    const int q_begin = EXT ? P.ext_off[pair] : P.sched_off[pair];
+    const int q_end = EXT ? P.ext_off[pair + 1] : P.sched_off[pair + 1];
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
@@ -143,13 +168,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
         bars->abort = 0;
         fence_mbar_init();
     }
-    if (warp == 0 && lane == 0) {
-        for (int i = 0; i < P.nstages; ++i) {
-            tma_prefetch_desc(&P.st[i].tm_w);
-            tma_prefetch_desc(&P.st[i].tm_x);
-            tma_prefetch_desc(&P.st[i].tm_wt);
-            tma_prefetch_desc(&P.st[i].tm_out);
-        }
+    if (warp == 0 && lane == 0) {  // descriptors of the stages in the parameters
+        for (int i = 0; i < kChainMaxStages && !EXT; ++i)
+            if (P.st[i].tiles_m) {
+                tma_prefetch_desc(&P.st[i].tm_w);
+                tma_prefetch_desc(&P.st[i].tm_x);
+                tma_prefetch_desc(&P.st[i].tm_wt);
+                tma_prefetch_desc(&P.st[i].tm_out);
+            }
     }
     if (warp == 1) tmem_alloc_pair(&bars->tmem_base, G::TMEM_COLS);
     tc_fence_before();
@@ -163,18 +189,20 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
             int s = 0;
             uint32_t ph = 0;
             uint32_t pending = 0, pending_ph = 0;
-            for (int q = P.sched_off[pair]; q < P.sched_off[pair + 1]; ++q) {
-                const int t = P.sched[q];
-                int si, mb, nb;
-                decode_item(P, t, si, mb, nb);
-                const ChainStage &cs = P.st[si];
+            for (int q = q_begin; q < q_end; ++q) {
+                const uint32_t e = entry_at<EXT>(P, q);
+                const int si = e >> 23, mb = (e >> 12) & 2047, nb = e & 4095;
+                const int t = q;
+                const ChainStage &cs = stage_at<EXT>(P, si);
                 const int M = cs.a.M, N = cs.a.N;
+                trace_put(P, t, rank, TR_ENTRY, e);
                 trace_put(P, t, rank, TR_SM, smid());
                 trace_put(P, t, rank, TR_PROD_START, globaltimer_ns());
-                if (si > 0) {
-                    // stage si-1 must have stored all of column block nb
-                    const int *cnt = P.done + (si - 1) * P.tiles_n + nb;
-                    const int need = kDoneIncrementsPerTile * P.st[si - 1].tiles_m;
+                if (cs.prev >= 0) {
+                    // the previous stage must have stored all of column block nb
+                    const ChainStage &ps = stage_at<EXT>(P, cs.prev);
+                    const int *cnt = P.done + ps.done_off + nb;
+                    const int need = kDoneIncrementsPerTile * ps.tiles_m;
                     if (ld_acquire_gpu(cnt) < need) {
                         const uint64_t t0 = globaltimer_ns();
                         while (ld_acquire_gpu(cnt) < need) {
@@ -204,7 +232,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
                         my_boxes = nbx;
                     }
                 }
+                // per-tile operands, kept in registers across the k-loop
                 const int num_kb = (cs.a.K + G::BK - 1) / G::BK;
+                const int ma = m0p + 128 * (int)rank;
+                const bool a_tail = my_a && tile_has_tail(cs.a, ma);
+                const CUtensorMap *tm_a = a_tail ? &cs.tm_wt : &cs.tm_w;
+                const CUtensorMap *tm_b = &cs.tm_x;
+                const int a_row = a_tail ? ma - cs.a.tail_row0 : ma;
+                const int b_col = n0 + (BN / 2) * (int)rank;
                 for (int kb = 0; kb < num_kb; ++kb) {
                     if (!mbar_wait(&bars->empty[s], ph ^ 1, status, KERR_WAIT_EMPTY)) {
                         set_abort(bars);
@@ -214,16 +249,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
                     const uint32_t full_leader = mapa_shared(smem_u32(&bars->full[s]), 0);
                     if (leader) mbar_arrive_expect_tx(&bars->full[s], (uint32_t)tx);
                     const int k0 = kb * G::BK;
-                    if (my_a) {
-                        const int ma = m0p + 128 * (int)rank;
-                        if (tile_has_tail(cs.a, ma))
-                            tma_load_2d_pair(st, &cs.tm_wt, full_leader, k0, ma - cs.a.tail_row0);
-                        else
-                            tma_load_2d_pair(st, &cs.tm_w, full_leader, k0, ma);
-                    }
+                    if (my_a) tma_load_2d_pair(st, tm_a, full_leader, k0, a_row);
                     for (int j = 0; j < my_boxes; ++j)
-                        tma_load_2d_pair(st + G::A_BYTES + j * G::BOX_BYTES, &cs.tm_x, full_leader,
-                                         n0 + (BN / 2) * (int)rank + j * G::BOX_N, k0);
+                        tma_load_2d_pair(st + G::A_BYTES + j * G::BOX_BYTES, tm_b, full_leader,
+                                         b_col + j * G::BOX_N, k0);
                     if (leader) {
                         pending |= 1u << s;
                         pending_ph = (pending_ph & ~(1u << s)) | (ph << s);
@@ -248,11 +277,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
             uint32_t ph = 0;
             int acc = 0;
             uint32_t acc_ph = 0;
-            for (int q = P.sched_off[pair]; q < P.sched_off[pair + 1]; ++q) {
-                const int t = P.sched[q];
-                int si, mb, nb;
-                decode_item(P, t, si, mb, nb);
-                const int num_kb = (P.st[si].a.K + G::BK - 1) / G::BK;
+            for (int q = q_begin; q < q_end; ++q) {
+                const int t = q;
+                const int si = entry_at<EXT>(P, q) >> 23;
+                const int num_kb = (stage_at<EXT>(P, si).a.K + G::BK - 1) / G::BK;
                 if (!mbar_wait(&bars->acc_empty[acc], acc_ph ^ 1, status, KERR_WAIT_ACC_EMPTY)) {
                     set_abort(bars);
                     break;
@@ -305,10 +333,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
         uint32_t acc_ph = 0;
         uint8_t *staging = smem + S * G::STAGE_BYTES + (warp - 2) * 2 * kStageBufBytes;
         int sbuf = 0;
-        for (int q = P.sched_off[pair]; q < P.sched_off[pair + 1]; ++q) {
-            const int t = P.sched[q];
-            int si, mb, nb;
-            decode_item(P, t, si, mb, nb);
+        for (int q = q_begin; q < q_end; ++q) {
+            const uint32_t e = entry_at<EXT>(P, q);
+            const int si = e >> 23, mb = (e >> 12) & 2047, nb = e & 4095;
+            const int t = q;
             if (!mbar_wait(&bars->acc_full[acc], acc_ph, status, KERR_WAIT_ACC_FULL)) {
                 set_abort(bars);
                 break;
@@ -318,8 +346,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
             const int m0 = mb * G::BM + 128 * (int)rank;
             const int n0 = nb * BN;
             const uint32_t t_row = tmem_base + acc * BN + ((uint32_t)(quarter * 32) << 16);
-            drain_warp<OP, BN>(P.st[si].a, &P.st[si].tm_out, t_row, lane, m0 + quarter * 32, n0,
-                               staging, sbuf);
+            const ChainStage &cs = stage_at<EXT>(P, si);
+            drain_warp<OP, BN>(cs.a, &cs.tm_out, t_row, lane, m0 + quarter * 32, n0, staging,
+                               sbuf);
             tc_fence_before();
             __threadfence();  // direct-store path: this lane's stores before the release
             __syncwarp();
@@ -330,7 +359,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
                 bulk_wait<0>();
                 fence_proxy_async_global();
                 __threadfence();
-                red_release_gpu_add(P.done + si * P.tiles_n + nb, 1);
+                red_release_gpu_add(P.done + cs.done_off + nb, 1);
                 if (quarter == 0) trace_put(P, t, rank, TR_EPI_END, globaltimer_ns());
             }
             if (++acc == 2) {
@@ -354,28 +383,89 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
 
 // ------------------------------------------------------------------ host side
 
+size_t chain_group_table_bytes(int nstages, long items)
+{
+    auto r = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    return r((size_t)nstages * sizeof(ChainStage)) + r((size_t)items * sizeof(uint32_t)) +
+           r((size_t)(kChainMaxPairs + 1) * sizeof(int));
+}
+
+namespace {
+
+struct SchedEntry {
+    std::vector<long> key;
+    std::vector<int> off;
+    std::vector<uint32_t> items;
+};
+
+// List schedule: work entries in dependency order; each goes to the pair that
+// frees up first, starting when that pair is free and the previous stage's
+// tiles of its column block have finished (estimated: k-blocks of MMA plus a
+// fixed per-tile epilogue / hand-off overhead, in units of one k-block).
+void build_schedule(const std::vector<ChainStage> &st, int pairs, int bk, std::vector<int> &off,
+                    std::vector<uint32_t> &items)
+{
+    const int n = (int)st.size();
+    std::vector<int> depth(n, 0), order(n);
+    for (int i = 0; i < n; ++i) depth[i] = st[i].prev < 0 ? 0 : depth[st[i].prev] + 1;
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return depth[x] < depth[y]; });
+    long nblocks = 0;
+    for (auto &c : st) nblocks = std::max<long>(nblocks, (long)c.done_off + c.tiles_n);
+    std::vector<double> block_done(nblocks, 0.0);
+    std::vector<double> pair_free(pairs, 0.0);
+    std::vector<std::vector<uint32_t>> per(pairs);
+    for (int si : order) {
+        const ChainStage &c = st[si];
+        const double cost = (double)((c.a.K + bk - 1) / bk) + 6.0;
+        for (int nb = 0; nb < c.tiles_n; ++nb)
+            for (int mb = 0; mb < c.tiles_m; ++mb) {
+                const double ready =
+                    c.prev >= 0 ? block_done[st[c.prev].done_off + nb] + 2.0 : 0.0;
+                // earliest start; among equal starts the lowest pair index
+                int best = 0;
+                double best_start = 1e300;
+                for (int p = 0; p < pairs; ++p) {
+                    const double t = pair_free[p] > ready ? pair_free[p] : ready;
+                    if (t < best_start - 1e-9) best_start = t, best = p;
+                }
+                const double fin = best_start + cost;
+                pair_free[best] = fin;
+                per[best].push_back(pack_item(si, mb, nb));
+                double &bd = block_done[c.done_off + nb];
+                if (fin > bd) bd = fin;
+            }
+    }
+    off.assign(pairs + 1, 0);
+    items.clear();
+    for (int p = 0; p < pairs; ++p) {
+        off[p + 1] = off[p] + (int)per[p].size();
+        items.insert(items.end(), per[p].begin(), per[p].end());
+    }
+}
+
+}  // namespace
+
 template <int OP>
-static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, int *status,
-                                   unsigned long long *trace, int num_sms, cudaStream_t s)
+static cudaError_t launch_group_op(const StageArgs *stages, const int *prev, int n, int *done,
+                                   int *status, unsigned long long *trace, void *ext_dev,
+                                   int num_sms, cudaStream_t s)
 {
     using T = OpTraits<OP>;
     using G = PairGeo<OP>;
-    static std::mutex mu;  // P and the schedule scratch are static (~28 KB): one launch at a time
+    static std::mutex mu;  // P (~28 KB) is static: one launch is built at a time
     std::lock_guard<std::mutex> lk(mu);
     static ChainParams P;
     memset(&P, 0, sizeof P);
     CUtensorMapDataType dt = OP == OP_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
                                            : CU_TENSOR_MAP_DATA_TYPE_UINT8;
-    const int N = stages[0].N;
-    P.nstages = n;
-    P.tiles_n = (N + G::BN - 1) / G::BN;
-    P.done = done;
-    P.status = status;
-    P.trace = trace;
-    int items = 0;
+    std::vector<ChainStage> st(n);
+    long items = 0;
+    int done_off = 0;
     for (int i = 0; i < n; ++i) {
         const StageArgs &a = stages[i];
-        ChainStage &cs = P.st[i];
+        ChainStage &cs = st[i];
+        memset(&cs, 0, sizeof cs);
         if (!make_map(&cs.tm_w, dt, T::elt, a.w, a.M, a.K, a.ld_w, G::BK, 128))
             return cudaErrorInvalidValue;
         if (!make_map(&cs.tm_x, dt, T::elt, a.x, a.K, a.N, a.ld_x, G::BOX_N, G::BK))
@@ -391,11 +481,16 @@ static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, in
         cs.a.tma_store = make_out_map(&cs.tm_out, cs.a) ? 1 : 0;
         if (!cs.a.tma_store) cs.tm_out = cs.tm_w;
         cs.tiles_m = (a.M + G::BM - 1) / G::BM;
-        cs.item0 = items;
-        items += cs.tiles_m * P.tiles_n;
+        cs.tiles_n = (a.N + G::BN - 1) / G::BN;
+        cs.prev = prev[i];
+        cs.done_off = done_off;
+        done_off += cs.tiles_n;
+        if (i >= 512 || cs.tiles_m > 2048 || cs.tiles_n > 4096 || (prev[i] >= i)) return cudaErrorNotSupported;
+        items += (long)cs.tiles_m * cs.tiles_n;
     }
-    P.total_items = items;
-    if (items > kChainMaxItems) return cudaErrorNotSupported;
+    P.done = done;
+    P.status = status;
+    P.trace = trace;
 
     static unsigned long long attr_set = 0;
     static int max_pairs[64];
@@ -415,12 +510,15 @@ static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, in
     cfg.attrs = attr;
     cfg.numAttrs = 1;  // occupancy query without the cooperative flag
     if (!(attr_set & (1ull << (dev & 63)))) {
-        cudaError_t e = cudaFuncSetAttribute(tc_chain_kernel<OP>,
+        cudaError_t e = cudaFuncSetAttribute(tc_chain_kernel<OP, false>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(tc_chain_kernel<OP, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES);
         if (e != cudaSuccess) return e;
         int clusters = 0;
         cfg.gridDim = dim3(2 * (num_sms / 2));
-        e = cudaOccupancyMaxActiveClusters(&clusters, tc_chain_kernel<OP>, &cfg);
+        e = cudaOccupancyMaxActiveClusters(&clusters, tc_chain_kernel<OP, false>, &cfg);
         if (e != cudaSuccess || clusters < 1) {
             cudaGetLastError();
             return cudaErrorNotSupported;
@@ -428,89 +526,84 @@ static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, in
         max_pairs[dev & 63] = clusters;
         attr_set |= 1ull << (dev & 63);
     }
-    int pairs = items < max_pairs[dev & 63] ? items : max_pairs[dev & 63];
+    int pairs = (int)std::min<long>(items, max_pairs[dev & 63]);
     if (pairs > kChainMaxPairs) pairs = kChainMaxPairs;
     P.npairs = pairs;
-    // The schedule depends only on the shapes: computed once per shape set.
-    struct Sched {
-        std::vector<long> key;
-        std::vector<uint16_t> off, items;
-    };
-    static std::vector<Sched> cache;
-    std::vector<long> key = {pairs, n, N};
+
+    // the schedule depends only on the shapes: computed once per shape set
+    static std::vector<SchedEntry> cache;
+    std::vector<long> key = {pairs, n};
     for (int i = 0; i < n; ++i) {
         key.push_back(stages[i].M);
         key.push_back(stages[i].K);
+        key.push_back(stages[i].N);
+        key.push_back(prev[i]);
     }
-    for (const Sched &c : cache)
-        if (c.key == key) {
-            memcpy(P.sched_off, c.off.data(), c.off.size() * sizeof(uint16_t));
-            memcpy(P.sched, c.items.data(), c.items.size() * sizeof(uint16_t));
-            cfg.gridDim = dim3(2 * pairs);
-            cfg.numAttrs = 2;
-            return cudaLaunchKernelEx(&cfg, tc_chain_kernel<OP>, P);
-        }
-    // List schedule in item order with estimated times: an item can start when
-    // its pair is free and the previous stage's tiles of its column block have
-    // finished; it goes to the pair that can start it first. Cost model: k-blocks
-    // of MMA plus a fixed per-tile epilogue / hand-off overhead (both in units
-    // of one k-block).
-    {
-        static double pair_free[kChainMaxPairs];
-        static double fin[kChainMaxItems];
-        static int owner[kChainMaxItems];
-        static double block_done[kChainMaxStages][1024];
-        int count[kChainMaxPairs];
-        const int tn = P.tiles_n < 1024 ? P.tiles_n : 1024;
-        for (int p = 0; p < pairs; ++p) pair_free[p] = 0.0, count[p] = 0;
-        for (int i = 0; i < n; ++i)
-            for (int b = 0; b < tn; ++b) block_done[i][b] = 0.0;
-        for (int t = 0; t < items; ++t) {
-            int si = 0;
-            while (si + 1 < n && t >= P.st[si + 1].item0) ++si;
-            const int u = t - P.st[si].item0;
-            const int nb = u / P.st[si].tiles_m;
-            const double cost = (double)((P.st[si].a.K + G::BK - 1) / G::BK) + 6.0;
-            const double ready = (si > 0 && nb < tn) ? block_done[si - 1][nb] + 2.0 : 0.0;
-            int best = 0;
-            double best_start = 1e300;
-            for (int p = 0; p < pairs; ++p) {
-                const double st = pair_free[p] > ready ? pair_free[p] : ready;
-                if (st < best_start - 1e-9) best_start = st, best = p;
-            }
-            fin[t] = best_start + cost;
-            pair_free[best] = fin[t];
-            owner[t] = best;
-            ++count[best];
-            if (nb < tn && fin[t] > block_done[si][nb]) block_done[si][nb] = fin[t];
-        }
-        P.sched_off[0] = 0;
-        for (int p = 0; p < pairs; ++p) P.sched_off[p + 1] = (uint16_t)(P.sched_off[p] + count[p]);
-        int fill[kChainMaxPairs];
-        for (int p = 0; p < pairs; ++p) fill[p] = P.sched_off[p];
-        for (int t = 0; t < items; ++t) P.sched[fill[owner[t]]++] = (uint16_t)t;
+    const SchedEntry *sc = nullptr;
+    for (const SchedEntry &c : cache)
+        if (c.key == key) sc = &c;
+    if (!sc) {
+        SchedEntry e;
+        e.key = key;
+        build_schedule(st, pairs, G::BK, e.off, e.items);
+        if (cache.size() >= 32) cache.erase(cache.begin());
+        cache.push_back(std::move(e));
+        sc = &cache.back();
     }
-    if (cache.size() >= 16) cache.erase(cache.begin());
-    cache.push_back(Sched{key, std::vector<uint16_t>(P.sched_off, P.sched_off + pairs + 1),
-                          std::vector<uint16_t>(P.sched, P.sched + items)});
+
+    if (n <= kChainMaxStages && items <= kParamSchedItems) {
+        for (int i = 0; i < n; ++i) P.st[i] = st[i];
+        for (int p = 0; p <= pairs; ++p) P.sched_off[p] = sc->off[p];
+        memcpy(P.sched, sc->items.data(), sc->items.size() * sizeof(uint32_t));
+        cfg.gridDim = dim3(2 * pairs);
+        cfg.numAttrs = 2;
+        return cudaLaunchKernelEx(&cfg, tc_chain_kernel<OP, false>, P);
+    } else {
+        if (!ext_dev) return cudaErrorNotSupported;
+        // tables in device memory: stages | entries | per-pair offsets
+        auto r = [](size_t b) { return (b + 255) & ~(size_t)255; };
+        const size_t b_st = r((size_t)n * sizeof(ChainStage));
+        const size_t b_it = r((size_t)items * sizeof(uint32_t));
+        std::vector<unsigned char> host(chain_group_table_bytes(n, items));
+        memcpy(host.data(), st.data(), (size_t)n * sizeof(ChainStage));
+        memcpy(host.data() + b_st, sc->items.data(), (size_t)items * sizeof(uint32_t));
+        memcpy(host.data() + b_st + b_it, sc->off.data(), (size_t)(pairs + 1) * sizeof(int));
+        cudaError_t e = cudaMemcpyAsync(ext_dev, host.data(), host.size(), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return e;
+        unsigned char *d = static_cast<unsigned char *>(ext_dev);
+        P.ext_st = reinterpret_cast<const ChainStage *>(d);
+        P.ext_sched = reinterpret_cast<const uint32_t *>(d + b_st);
+        P.ext_off = reinterpret_cast<const int *>(d + b_st + b_it);
+    }
     cfg.gridDim = dim3(2 * pairs);
     cfg.numAttrs = 2;
-    return cudaLaunchKernelEx(&cfg, tc_chain_kernel<OP>, P);
+    return cudaLaunchKernelEx(&cfg, tc_chain_kernel<OP, true>, P);
+}
+
+cudaError_t launch_tc_group(const StageArgs *stages, const int *prev, int n, int *done,
+                            int *status, unsigned long long *trace, void *ext_dev, int num_sms,
+                            cudaStream_t s)
+{
+    if (n < 1) return cudaErrorInvalidValue;
+    for (int i = 0; i < n; ++i)
+        if (stages[i].op != stages[0].op || stages[i].M <= 0 || stages[i].K <= 0 ||
+            stages[i].N <= 0)
+            return cudaErrorInvalidValue;
+    switch (stages[0].op) {
+    case OP_BF16:
+        return launch_group_op<OP_BF16>(stages, prev, n, done, status, trace, ext_dev, num_sms, s);
+    case OP_I8:
+        return launch_group_op<OP_I8>(stages, prev, n, done, status, trace, ext_dev, num_sms, s);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_tc_chain(const StageArgs *stages, int n, int *done, int *status,
                             unsigned long long *trace, int num_sms, cudaStream_t s)
 {
-    if (n < 1 || n > kChainMaxStages) return cudaErrorInvalidValue;
-    for (int i = 0; i < n; ++i)
-        if (stages[i].op != stages[0].op || stages[i].N != stages[0].N || stages[i].M <= 0 ||
-            stages[i].K <= 0)
-            return cudaErrorInvalidValue;
-    switch (stages[0].op) {
-    case OP_BF16: return launch_chain_op<OP_BF16>(stages, n, done, status, trace, num_sms, s);
-    case OP_I8: return launch_chain_op<OP_I8>(stages, n, done, status, trace, num_sms, s);
-    default: return cudaErrorInvalidValue;
-    }
+    std::vector<int> prev(n);
+    for (int i = 0; i < n; ++i) prev[i] = i - 1;
+    return launch_tc_group(stages, prev.data(), n, done, status, trace, nullptr, num_sms, s);
 }
 
 int chain_max_stages() { return kChainMaxStages; }

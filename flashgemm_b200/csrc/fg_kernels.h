@@ -57,6 +57,16 @@ cudaError_t launch_tc_chain(const StageArgs *stages, int n, int *done, int *stat
 int chain_max_stages();
 int chain_trace_fields();
 
+// Several chains of one op in one launch: stage i reads the output of stage
+// prev[i] (-1: a chain's first stage; prev[i] < i). `done` holds
+// sum_i ceil(N_i / 256) zeroed ints; ext_dev (device memory of
+// chain_group_table_bytes(n, work entries) bytes, or null) holds the stage table
+// and schedule when they do not fit in the kernel parameters.
+cudaError_t launch_tc_group(const StageArgs *stages, const int *prev, int n, int *done,
+                            int *status, unsigned long long *trace, void *ext_dev, int num_sms,
+                            cudaStream_t s);
+size_t chain_group_table_bytes(int nstages, long items);
+
 // Plain FP32 SGEMM on CUDA cores: C = A * B, one FMA per k in increasing k;
 // with kblock > 0 each block of kblock k is summed from zero and added to C.
 struct FfmaArgs {

@@ -108,6 +108,24 @@ int fg_weights_release(fg_weights w);
 int fg_chain_registered(int dtype, void *C, const void *B, long N, int num_gemm,
                         const fg_weights *W, void *stream);
 
+/* One chain of a grouped launch: device B (K_0 x N) and C (M_{n-1} x N) with
+ * dense rows (N * element size a multiple of 16 bytes), registered weights. */
+typedef struct {
+    void *C;
+    const void *B;
+    long N;
+    int num_gemm;
+    const fg_weights *W;
+} fg_chain_desc;
+
+/* Many independent chains of one dtype in ONE persistent launch (BF16, INT8):
+ * the CTA pairs of the grid walk all chains' tiles together under a schedule
+ * the host computes per shape set (cached), each chain's stages ordered by
+ * their per-block completion counters. Chains of uneven lengths and shapes mix
+ * freely. FP32 chains (no grouped FP32 kernel) run one after another.
+ * Asynchronous, ordered on `stream` like fg_chain_dev. */
+int fg_chain_group(int dtype, int nchains, const fg_chain_desc *chains, void *stream);
+
 /* Wait for all of the library's work on the current device and report any
  * kernel-side error since the last fg_sync (then cleared). */
 int fg_sync(void);

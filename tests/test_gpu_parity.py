@@ -327,3 +327,39 @@ def test_registered_weights_match_per_call_weights(fg, dt, f32algo):
             w.release()
     finally:
         fg.set_f32_algo("3xtf32")
+
+
+@pytest.mark.parametrize("dt", ["int8", "bf16"])
+def test_grouped_launch_matches_chains_run_alone(fg, dt):
+    """Chains of uneven lengths and shapes in one grouped launch (more stages
+    than fit in the kernel parameters, so the tables go through device memory)
+    give exactly what each chain gives on its own."""
+    import torch
+    rng = np.random.default_rng(5)
+    specs = []
+    for j in range(7):
+        n = int(rng.integers(2, 5))
+        N = int(rng.choice([256, 512, 768, 1280]))
+        dims = [int(rng.choice([64, 128, 272, 520, 1024]))] + \
+               [int(rng.choice([128, 260, 384, 1000])) for _ in range(n)]
+        if dt == "int8":
+            dims[0] = max(64, dims[0] // 32 * 32)
+        specs.append((N, dims[0], dims[1:]))
+    chains, alone = [], []
+    for j, (N, K1, Ms) in enumerate(specs):
+        B, As, Ks = oracle.chain_inputs(dt, N, K1, Ms, seed=100 + j)
+        W = [fg.Weights(dt, a) for a in As]
+        tB = torch.from_numpy(B.view(np.int8) if dt == "int8" else B.view(np.int16)).cuda()
+        mk = lambda: torch.zeros((Ms[-1], N), dtype=torch.int32 if dt == "int8" else torch.float32,
+                                 device="cuda")
+        c1, c2 = mk(), mk()
+        fg.chain_registered(dt, c1, tB, N, W)
+        chains.append((c2, tB, N, W))
+        alone.append(c1)
+    fg.chain_group(dt, chains)
+    torch.cuda.synchronize()
+    fg.sync()
+    for (c2, _, _, W), c1 in zip(chains, alone):
+        np.testing.assert_array_equal(c2.cpu().numpy(), c1.cpu().numpy())
+        for w in W:
+            w.release()
