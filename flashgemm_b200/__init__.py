@@ -325,12 +325,7 @@ class _ChainDesc(ctypes.Structure):
     _fields_ = [("C", _P), ("B", _P), ("N", _L), ("num_gemm", ctypes.c_int), ("W", _P)]
 
 
-def chain_group(dtype, chains, stream=None):
-    """Many chains in one persistent launch. chains: list of (C, B, N, [Weights])
-    with torch CUDA tensors for C and B."""
-    import torch
-    L = lib()
-    L.fg_chain_group.argtypes = [ctypes.c_int, ctypes.c_int, _P, _P]
+def _descs(chains):
     keep = []
     descs = (_ChainDesc * len(chains))()
     for d, (C, B, N, W) in zip(descs, chains):
@@ -338,7 +333,127 @@ def chain_group(dtype, chains, stream=None):
         keep.append(hs)
         d.C, d.B, d.N, d.num_gemm = C.data_ptr(), B.data_ptr(), int(N), len(W)
         d.W = ctypes.cast(hs, _P)
+    return descs, keep
+
+
+def chain_group(dtype, chains, stream=None):
+    """Many chains in one grouped launch. chains: list of (C, B, N, [Weights])
+    with torch CUDA tensors for C and B."""
+    import torch
+    L = lib()
+    L.fg_chain_group.argtypes = [ctypes.c_int, ctypes.c_int, _P, _P]
+    descs, keep = _descs(chains)
     s = (stream or torch.cuda.current_stream()).cuda_stream
     st = L.fg_chain_group(_DT[dtype], len(chains), ctypes.cast(descs, _P), s)
     if st != FG_OK:
         raise FlashgemmError(st, last_error())
+
+
+FG_GROUP_AUTO, FG_GROUP_PAIR, FG_GROUP_SINGLE_256, FG_GROUP_SINGLE_128 = -1, 0, 1, 2
+FG_ORDER_AUTO, FG_ORDER_FUSED, FG_ORDER_LEVELS = -1, 0, 1
+
+
+def set_group_config(kernel=FG_GROUP_AUTO, order=FG_ORDER_AUTO):
+    """Kernel (FG_GROUP_*) and stage order (FG_ORDER_*) of later grouped launches."""
+    L = lib()
+    L.fg_set_group_config.restype = None
+    L.fg_set_group_config(int(kernel), int(order))
+
+
+def get_group_config():
+    L = lib()
+    k, o = ctypes.c_int(), ctypes.c_int()
+    L.fg_get_group_config.restype = None
+    L.fg_get_group_config(ctypes.byref(k), ctypes.byref(o))
+    return k.value, o.value
+
+
+def group_choice(dtype, chains):
+    """(kernel, order) a grouped launch of these chains would use now."""
+    L = lib()
+    descs, keep = _descs(chains)
+    k, o = ctypes.c_int(), ctypes.c_int()
+    L.fg_group_choice.argtypes = [ctypes.c_int, ctypes.c_int, _P, _P, _P]
+    st = L.fg_group_choice(_DT[dtype], len(chains), ctypes.cast(descs, _P), ctypes.byref(k),
+                           ctypes.byref(o))
+    if st != FG_OK:
+        raise FlashgemmError(st, last_error())
+    return k.value, o.value
+
+
+def autotune_group(dtype, chains, iters=3):
+    """Time every kernel / order candidate on this group; returns (kernel, order, ms)
+    and remembers the choice for groups of the same shapes."""
+    L = lib()
+    descs, keep = _descs(chains)
+    k, o, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+    L.fg_autotune_group.argtypes = [ctypes.c_int, ctypes.c_int, _P, ctypes.c_int, _P, _P, _P]
+    st = L.fg_autotune_group(_DT[dtype], len(chains), ctypes.cast(descs, _P), int(iters),
+                             ctypes.byref(k), ctypes.byref(o), ctypes.byref(ms))
+    if st != FG_OK:
+        raise FlashgemmError(st, last_error())
+    return k.value, o.value, ms.value
+
+
+def autotune_save(path):
+    L = lib()
+    L.fg_autotune_save.argtypes = [ctypes.c_char_p]
+    if L.fg_autotune_save(str(path).encode()) != FG_OK:
+        raise FlashgemmError(last_status(), last_error())
+
+
+def autotune_load(path):
+    L = lib()
+    L.fg_autotune_load.argtypes = [ctypes.c_char_p]
+    if L.fg_autotune_load(str(path).encode()) != FG_OK:
+        raise FlashgemmError(last_status(), last_error())
+
+
+class Plan:
+    """A planned grouped launch bound to its chains' buffers (fg_plan_create)."""
+
+    def __init__(self, dtype, chains):
+        L = lib()
+        descs, keep = _descs(chains)
+        h = _P()
+        L.fg_plan_create.argtypes = [ctypes.c_int, ctypes.c_int, _P, _P]
+        st = L.fg_plan_create(_DT[dtype], len(chains), ctypes.cast(descs, _P), ctypes.byref(h))
+        if st != FG_OK:
+            raise FlashgemmError(st, last_error())
+        self.handle = h.value
+        self._chains = chains  # the plan points at these tensors
+
+    def launch(self, stream=None, graph=False):
+        import torch
+        L = lib()
+        s = (stream or torch.cuda.current_stream()).cuda_stream
+        f = L.fg_plan_launch_graph if graph else L.fg_plan_launch
+        f.argtypes = [_P, _P]
+        st = f(self.handle, s)
+        if st != FG_OK:
+            raise FlashgemmError(st, last_error())
+
+    def info(self):
+        """dict(kernel, order, device_bytes, kernels, flops)."""
+        L = lib()
+        k, o, b, n, fl = ctypes.c_int(), ctypes.c_int(), _L(), ctypes.c_int(), ctypes.c_double()
+        L.fg_plan_info.argtypes = [_P, _P, _P, _P, _P, _P]
+        st = L.fg_plan_info(self.handle, ctypes.byref(k), ctypes.byref(o), ctypes.byref(b),
+                            ctypes.byref(n), ctypes.byref(fl))
+        if st != FG_OK:
+            raise FlashgemmError(st, last_error())
+        return dict(kernel=k.value, order=o.value, device_bytes=b.value, kernels=n.value,
+                    flops=fl.value)
+
+    def release(self):
+        if self.handle:
+            L = lib()
+            L.fg_plan_release.argtypes = [_P]
+            L.fg_plan_release(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass

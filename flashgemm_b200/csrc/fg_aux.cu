@@ -41,6 +41,32 @@ cudaError_t launch_split_tf32(const float *in, long ld_in, float *hi, float *lo,
     return cudaGetLastError();
 }
 
+// Many splits in one launch: blockIdx.y = job.
+__global__ void split_tf32_jobs_kernel(const SplitJob *__restrict__ jobs)
+{
+    const SplitJob j = jobs[blockIdx.y];
+    const long total = j.rows * j.cols;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+         i += (long)gridDim.x * blockDim.x) {
+        const long r = i / j.cols, c = i - r * j.cols;
+        const float x = j.in[r * j.ld_in + c];
+        const float h = tf32_rne(x);
+        j.hi[r * j.ld_out + c] = h;
+        j.lo[r * j.ld_out + c] = tf32_rne(x - h);
+    }
+}
+
+cudaError_t launch_split_tf32_jobs(const SplitJob *jobs_dev, int njobs, long max_elems,
+                                   cudaStream_t s)
+{
+    if (njobs < 1 || max_elems < 1) return cudaSuccess;
+    if (njobs > 65535) return cudaErrorInvalidValue;
+    long blocks = (max_elems + 255) / 256;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    split_tf32_jobs_kernel<<<dim3((unsigned)blocks, (unsigned)njobs), 256, 0, s>>>(jobs_dev);
+    return cudaGetLastError();
+}
+
 // Rows m in [tail_lo, tail_hi) of the reference's INT8 chain meet activation
 // k-quad max(s-1, 0) with weight k-quad s (multigemm/src/kernel_int8.h:405 vs
 // :427, :590 vs :608). The prepared copy shifts those rows left by one quad,

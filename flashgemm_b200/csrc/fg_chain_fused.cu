@@ -62,7 +62,7 @@ __host__ __device__ constexpr uint32_t pack_item(int stage, int mb, int nb)
 struct ChainParams {
     ChainStage st[kChainMaxStages];
     const ChainStage *ext_st;
-    const uint32_t *ext_sched;
+    const WorkEntry *ext_sched;
     const int *ext_off;
     int npairs;
     int *done;        // per (stage, column block): epilogue warps that finished a tile
@@ -72,24 +72,6 @@ struct ChainParams {
     uint32_t sched[kParamSchedItems];
 };
 static_assert(sizeof(ChainParams) <= 32000, "kernel parameter space");
-
-__device__ __forceinline__ int ld_acquire_gpu(const int *p)
-{
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void red_release_gpu_add(int *p, int v)
-{
-    asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// Generic-proxy writes / reads of global memory ordered with async-proxy (TMA) accesses.
-__device__ __forceinline__ void fence_proxy_async_global()
-{
-    asm volatile("fence.proxy.async.global;" ::: "memory");
-}
 
 // Trace record of one (item, CTA): where the time of a fused chain goes.
 enum { TR_ENTRY = 0, TR_SM, TR_PROD_START, TR_DEP_DONE, TR_PROD_END, TR_MMA_START, TR_MMA_END,
@@ -123,12 +105,19 @@ __device__ __forceinline__ const ChainStage &stage_at(const ChainParams &P, int 
 }
 
 template <bool EXT>
-__device__ __forceinline__ uint32_t entry_at(const ChainParams &P, int q)
+__device__ __forceinline__ void entry_at(const ChainParams &P, int q, int &si, int &mb, int &nb)
 {
-    if constexpr (EXT)
-        return P.ext_sched[q];
-    else
-        return P.sched[q];
+    if constexpr (EXT) {
+        const WorkEntry e = P.ext_sched[q];
+        si = (int)e.stage;
+        mb = (int)(e.mbnb >> 16);
+        nb = (int)(e.mbnb & 0xffffu);
+    } else {
+        const uint32_t e = P.sched[q];
+        si = (int)(e >> 23);
+        mb = (int)((e >> 12) & 2047u);
+        nb = (int)(e & 4095u);
+    }
 }
 
 // EXT: stage table and schedule in device memory (grouped launches) rather
@@ -190,12 +179,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
             uint32_t ph = 0;
             uint32_t pending = 0, pending_ph = 0;
             for (int q = q_begin; q < q_end; ++q) {
-                const uint32_t e = entry_at<EXT>(P, q);
-                const int si = e >> 23, mb = (e >> 12) & 2047, nb = e & 4095;
+                int si, mb, nb;
+                entry_at<EXT>(P, q, si, mb, nb);
                 const int t = q;
                 const ChainStage &cs = stage_at<EXT>(P, si);
                 const int M = cs.a.M, N = cs.a.N;
-                trace_put(P, t, rank, TR_ENTRY, e);
+                trace_put(P, t, rank, TR_ENTRY, pack_item(si, mb, nb));
                 trace_put(P, t, rank, TR_SM, smid());
                 trace_put(P, t, rank, TR_PROD_START, globaltimer_ns());
                 if (cs.prev >= 0) {
@@ -279,7 +268,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
             uint32_t acc_ph = 0;
             for (int q = q_begin; q < q_end; ++q) {
                 const int t = q;
-                const int si = entry_at<EXT>(P, q) >> 23;
+                int si, mb, nb;
+                entry_at<EXT>(P, q, si, mb, nb);
                 const int num_kb = (stage_at<EXT>(P, si).a.K + G::BK - 1) / G::BK;
                 if (!mbar_wait(&bars->acc_empty[acc], acc_ph ^ 1, status, KERR_WAIT_ACC_EMPTY)) {
                     set_abort(bars);
@@ -334,8 +324,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
         uint8_t *staging = smem + S * G::STAGE_BYTES + (warp - 2) * 2 * kStageBufBytes;
         int sbuf = 0;
         for (int q = q_begin; q < q_end; ++q) {
-            const uint32_t e = entry_at<EXT>(P, q);
-            const int si = e >> 23, mb = (e >> 12) & 2047, nb = e & 4095;
+            int si, mb, nb;
+            entry_at<EXT>(P, q, si, mb, nb);
             const int t = q;
             if (!mbar_wait(&bars->acc_full[acc], acc_ph, status, KERR_WAIT_ACC_FULL)) {
                 set_abort(bars);
@@ -383,206 +373,180 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
 
 // ------------------------------------------------------------------ host side
 
-size_t chain_group_table_bytes(int nstages, long items)
-{
-    auto r = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    return r((size_t)nstages * sizeof(ChainStage)) + r((size_t)items * sizeof(uint32_t)) +
-           r((size_t)(kChainMaxPairs + 1) * sizeof(int));
-}
-
 namespace {
 
-struct SchedEntry {
-    std::vector<long> key;
-    std::vector<int> off;
-    std::vector<uint32_t> items;
-};
-
-// List schedule: work entries in dependency order; each goes to the pair that
-// frees up first, starting when that pair is free and the previous stage's
-// tiles of its column block have finished (estimated: k-blocks of MMA plus a
-// fixed per-tile epilogue / hand-off overhead, in units of one k-block).
-void build_schedule(const std::vector<ChainStage> &st, int pairs, int bk, std::vector<int> &off,
-                    std::vector<uint32_t> &items)
-{
-    const int n = (int)st.size();
-    std::vector<int> depth(n, 0), order(n);
-    for (int i = 0; i < n; ++i) depth[i] = st[i].prev < 0 ? 0 : depth[st[i].prev] + 1;
-    for (int i = 0; i < n; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return depth[x] < depth[y]; });
-    long nblocks = 0;
-    for (auto &c : st) nblocks = std::max<long>(nblocks, (long)c.done_off + c.tiles_n);
-    std::vector<double> block_done(nblocks, 0.0);
-    std::vector<double> pair_free(pairs, 0.0);
-    std::vector<std::vector<uint32_t>> per(pairs);
-    for (int si : order) {
-        const ChainStage &c = st[si];
-        const double cost = (double)((c.a.K + bk - 1) / bk) + 6.0;
-        for (int nb = 0; nb < c.tiles_n; ++nb)
-            for (int mb = 0; mb < c.tiles_m; ++mb) {
-                const double ready =
-                    c.prev >= 0 ? block_done[st[c.prev].done_off + nb] + 2.0 : 0.0;
-                // earliest start; among equal starts the lowest pair index
-                int best = 0;
-                double best_start = 1e300;
-                for (int p = 0; p < pairs; ++p) {
-                    const double t = pair_free[p] > ready ? pair_free[p] : ready;
-                    if (t < best_start - 1e-9) best_start = t, best = p;
-                }
-                const double fin = best_start + cost;
-                pair_free[best] = fin;
-                per[best].push_back(pack_item(si, mb, nb));
-                double &bd = block_done[c.done_off + nb];
-                if (fin > bd) bd = fin;
-            }
-    }
-    off.assign(pairs + 1, 0);
-    items.clear();
-    for (int p = 0; p < pairs; ++p) {
-        off[p + 1] = off[p] + (int)per[p].size();
-        items.insert(items.end(), per[p].begin(), per[p].end());
-    }
-}
-
-}  // namespace
-
+// Stage table entry of one stage (tensor maps, shapes, dependencies).
 template <int OP>
-static cudaError_t launch_group_op(const StageArgs *stages, const int *prev, int n, int *done,
-                                   int *status, unsigned long long *trace, void *ext_dev,
-                                   int num_sms, cudaStream_t s)
+cudaError_t make_chain_stage(const StageArgs &a, int prev, int done_off, ChainStage &cs)
 {
     using T = OpTraits<OP>;
     using G = PairGeo<OP>;
-    static std::mutex mu;  // P (~28 KB) is static: one launch is built at a time
-    std::lock_guard<std::mutex> lk(mu);
-    static ChainParams P;
-    memset(&P, 0, sizeof P);
-    CUtensorMapDataType dt = OP == OP_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
-                                           : CU_TENSOR_MAP_DATA_TYPE_UINT8;
-    std::vector<ChainStage> st(n);
-    long items = 0;
-    int done_off = 0;
-    for (int i = 0; i < n; ++i) {
-        const StageArgs &a = stages[i];
-        ChainStage &cs = st[i];
-        memset(&cs, 0, sizeof cs);
-        if (!make_map(&cs.tm_w, dt, T::elt, a.w, a.M, a.K, a.ld_w, G::BK, 128))
+    const CUtensorMapDataType dt = OP == OP_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                 : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+    memset(&cs, 0, sizeof cs);
+    if (!make_map(&cs.tm_w, dt, T::elt, a.w, a.M, a.K, a.ld_w, G::BK, 128))
+        return cudaErrorInvalidValue;
+    if (!make_map(&cs.tm_x, dt, T::elt, a.x, a.K, a.N, a.ld_x, G::BOX_N, G::BK))
+        return cudaErrorInvalidValue;
+    if (a.tail_hi > a.tail_lo) {
+        if (!make_map(&cs.tm_wt, dt, T::elt, a.w_tail, a.M - a.tail_row0, a.K, a.ld_w_tail, G::BK,
+                      128))
             return cudaErrorInvalidValue;
-        if (!make_map(&cs.tm_x, dt, T::elt, a.x, a.K, a.N, a.ld_x, G::BOX_N, G::BK))
-            return cudaErrorInvalidValue;
-        if (a.tail_hi > a.tail_lo) {
-            if (!make_map(&cs.tm_wt, dt, T::elt, a.w_tail, a.M - a.tail_row0, a.K, a.ld_w_tail,
-                          G::BK, 128))
-                return cudaErrorInvalidValue;
-        } else {
-            cs.tm_wt = cs.tm_w;
-        }
-        cs.a = a;
-        cs.a.tma_store = make_out_map(&cs.tm_out, cs.a) ? 1 : 0;
-        if (!cs.a.tma_store) cs.tm_out = cs.tm_w;
-        cs.tiles_m = (a.M + G::BM - 1) / G::BM;
-        cs.tiles_n = (a.N + G::BN - 1) / G::BN;
-        cs.prev = prev[i];
-        cs.done_off = done_off;
-        done_off += cs.tiles_n;
-        if (i >= 512 || cs.tiles_m > 2048 || cs.tiles_n > 4096 || (prev[i] >= i)) return cudaErrorNotSupported;
-        items += (long)cs.tiles_m * cs.tiles_n;
+    } else {
+        cs.tm_wt = cs.tm_w;
     }
-    P.done = done;
-    P.status = status;
-    P.trace = trace;
+    cs.a = a;
+    cs.a.tma_store = make_out_map(&cs.tm_out, cs.a) ? 1 : 0;
+    if (!cs.a.tma_store) cs.tm_out = cs.tm_w;
+    cs.tiles_m = (a.M + G::BM - 1) / G::BM;
+    cs.tiles_n = (a.N + G::BN - 1) / G::BN;
+    cs.prev = prev;
+    cs.done_off = done_off;
+    if (cs.tiles_m > 65535 || cs.tiles_n > 65535) return cudaErrorNotSupported;
+    return cudaSuccess;
+}
 
-    static unsigned long long attr_set = 0;
-    static int max_pairs[64];
+// Pairs that fit on the device at once (cluster occupancy of the kernel), per device.
+template <int OP>
+cudaError_t pair_capacity(int num_sms, int &pairs)
+{
+    using G = PairGeo<OP>;
+    static std::mutex mu;
+    static int cap[64];
+    static unsigned long long known = 0;
+    std::lock_guard<std::mutex> lk(mu);
     int dev = 0;
     cudaGetDevice(&dev);
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute attr[2];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = 2;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    attr[1].id = cudaLaunchAttributeCooperative;
-    attr[1].val.cooperative = 1;
-    cfg.blockDim = dim3(kThreads);
-    cfg.dynamicSmemBytes = G::SMEM_BYTES;
-    cfg.stream = s;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;  // occupancy query without the cooperative flag
-    if (!(attr_set & (1ull << (dev & 63)))) {
+    if (!(known & (1ull << (dev & 63)))) {
         cudaError_t e = cudaFuncSetAttribute(tc_chain_kernel<OP, false>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(tc_chain_kernel<OP, true>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES);
         if (e != cudaSuccess) return e;
-        int clusters = 0;
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = G::SMEM_BYTES;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
         cfg.gridDim = dim3(2 * (num_sms / 2));
+        int clusters = 0;
         e = cudaOccupancyMaxActiveClusters(&clusters, tc_chain_kernel<OP, false>, &cfg);
         if (e != cudaSuccess || clusters < 1) {
             cudaGetLastError();
             return cudaErrorNotSupported;
         }
-        max_pairs[dev & 63] = clusters;
-        attr_set |= 1ull << (dev & 63);
+        cap[dev & 63] = clusters < kChainMaxPairs ? clusters : kChainMaxPairs;
+        known |= 1ull << (dev & 63);
     }
-    int pairs = (int)std::min<long>(items, max_pairs[dev & 63]);
-    if (pairs > kChainMaxPairs) pairs = kChainMaxPairs;
+    pairs = cap[dev & 63];
+    return cudaSuccess;
+}
+
+template <int OP, bool EXT>
+cudaError_t launch_pairs(const ChainParams &P, int pairs, cudaStream_t s)
+{
+    using G = PairGeo<OP>;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeCooperative;  // all pairs resident: they wait on one another
+    attr[1].val.cooperative = 1;
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = G::SMEM_BYTES;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 2;
+    cfg.gridDim = dim3(2 * pairs);
+    return cudaLaunchKernelEx(&cfg, tc_chain_kernel<OP, EXT>, P);
+}
+
+std::vector<SchedStage> sched_stages(const std::vector<ChainStage> &st, int bk)
+{
+    std::vector<SchedStage> ss(st.size());
+    for (size_t i = 0; i < st.size(); ++i)
+        ss[i] = SchedStage{st[i].tiles_m, st[i].tiles_n, st[i].prev, st[i].done_off,
+                           (double)((st[i].a.K + bk - 1) / bk) + 6.0};
+    return ss;
+}
+
+}  // namespace
+
+// One chain (stage i reads stage i - 1) with its tables in the kernel parameters.
+template <int OP>
+static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, int *status,
+                                   unsigned long long *trace, int num_sms, cudaStream_t s)
+{
+    using G = PairGeo<OP>;
+    if (n > kChainMaxStages) return cudaErrorNotSupported;
+    static std::mutex mu;  // P (~28 KB) is static: one launch is built at a time
+    std::lock_guard<std::mutex> lk(mu);
+    static ChainParams P;
+    memset(&P, 0, sizeof P);
+    std::vector<ChainStage> st(n);
+    long items = 0;
+    int done_off = 0;
+    for (int i = 0; i < n; ++i) {
+        cudaError_t e = make_chain_stage<OP>(stages[i], i - 1, done_off, st[i]);
+        if (e != cudaSuccess) return e;
+        if (st[i].tiles_m > 2047 || st[i].tiles_n > 4095) return cudaErrorNotSupported;
+        done_off += st[i].tiles_n;
+        items += (long)st[i].tiles_m * st[i].tiles_n;
+    }
+    if (items > kParamSchedItems) return cudaErrorNotSupported;
+    int pairs = 0;
+    cudaError_t e = pair_capacity<OP>(num_sms, pairs);
+    if (e != cudaSuccess) return e;
+    if (items < pairs) pairs = (int)items;
     P.npairs = pairs;
+    P.done = done;
+    P.status = status;
+    P.trace = trace;
 
     // the schedule depends only on the shapes: computed once per shape set
-    static std::vector<SchedEntry> cache;
+    struct Cached {
+        std::vector<long> key;
+        std::vector<int> off;
+        std::vector<uint32_t> items;
+    };
+    static std::vector<Cached> cache;
     std::vector<long> key = {pairs, n};
     for (int i = 0; i < n; ++i) {
         key.push_back(stages[i].M);
         key.push_back(stages[i].K);
         key.push_back(stages[i].N);
-        key.push_back(prev[i]);
     }
-    const SchedEntry *sc = nullptr;
-    for (const SchedEntry &c : cache)
+    const Cached *sc = nullptr;
+    for (const Cached &c : cache)
         if (c.key == key) sc = &c;
     if (!sc) {
-        SchedEntry e;
-        e.key = key;
-        build_schedule(st, pairs, G::BK, e.off, e.items);
+        Cached c;
+        c.key = key;
+        std::vector<WorkEntry> ent;
+        const std::vector<SchedStage> ss = sched_stages(st, G::BK);
+        list_schedule(ss.data(), n, pairs, 2.0, c.off, ent);
+        for (const WorkEntry &w : ent)
+            c.items.push_back(pack_item((int)w.stage, (int)(w.mbnb >> 16), (int)(w.mbnb & 0xffffu)));
         if (cache.size() >= 32) cache.erase(cache.begin());
-        cache.push_back(std::move(e));
+        cache.push_back(std::move(c));
         sc = &cache.back();
     }
-
-    if (n <= kChainMaxStages && items <= kParamSchedItems) {
-        for (int i = 0; i < n; ++i) P.st[i] = st[i];
-        for (int p = 0; p <= pairs; ++p) P.sched_off[p] = sc->off[p];
-        memcpy(P.sched, sc->items.data(), sc->items.size() * sizeof(uint32_t));
-        cfg.gridDim = dim3(2 * pairs);
-        cfg.numAttrs = 2;
-        return cudaLaunchKernelEx(&cfg, tc_chain_kernel<OP, false>, P);
-    } else {
-        if (!ext_dev) return cudaErrorNotSupported;
-        // tables in device memory: stages | entries | per-pair offsets
-        auto r = [](size_t b) { return (b + 255) & ~(size_t)255; };
-        const size_t b_st = r((size_t)n * sizeof(ChainStage));
-        const size_t b_it = r((size_t)items * sizeof(uint32_t));
-        std::vector<unsigned char> host(chain_group_table_bytes(n, items));
-        memcpy(host.data(), st.data(), (size_t)n * sizeof(ChainStage));
-        memcpy(host.data() + b_st, sc->items.data(), (size_t)items * sizeof(uint32_t));
-        memcpy(host.data() + b_st + b_it, sc->off.data(), (size_t)(pairs + 1) * sizeof(int));
-        cudaError_t e = cudaMemcpyAsync(ext_dev, host.data(), host.size(), cudaMemcpyHostToDevice, s);
-        if (e != cudaSuccess) return e;
-        unsigned char *d = static_cast<unsigned char *>(ext_dev);
-        P.ext_st = reinterpret_cast<const ChainStage *>(d);
-        P.ext_sched = reinterpret_cast<const uint32_t *>(d + b_st);
-        P.ext_off = reinterpret_cast<const int *>(d + b_st + b_it);
-    }
-    cfg.gridDim = dim3(2 * pairs);
-    cfg.numAttrs = 2;
-    return cudaLaunchKernelEx(&cfg, tc_chain_kernel<OP, true>, P);
+    for (int i = 0; i < n; ++i) P.st[i] = st[i];
+    for (int p = 0; p <= pairs; ++p) P.sched_off[p] = sc->off[p];
+    memcpy(P.sched, sc->items.data(), sc->items.size() * sizeof(uint32_t));
+    return launch_pairs<OP, false>(P, pairs, s);
 }
 
-cudaError_t launch_tc_group(const StageArgs *stages, const int *prev, int n, int *done,
-                            int *status, unsigned long long *trace, void *ext_dev, int num_sms,
-                            cudaStream_t s)
+cudaError_t launch_tc_chain(const StageArgs *stages, int n, int *done, int *status,
+                            unsigned long long *trace, int num_sms, cudaStream_t s)
 {
     if (n < 1) return cudaErrorInvalidValue;
     for (int i = 0; i < n; ++i)
@@ -590,20 +554,86 @@ cudaError_t launch_tc_group(const StageArgs *stages, const int *prev, int n, int
             stages[i].N <= 0)
             return cudaErrorInvalidValue;
     switch (stages[0].op) {
-    case OP_BF16:
-        return launch_group_op<OP_BF16>(stages, prev, n, done, status, trace, ext_dev, num_sms, s);
-    case OP_I8:
-        return launch_group_op<OP_I8>(stages, prev, n, done, status, trace, ext_dev, num_sms, s);
+    case OP_BF16: return launch_chain_op<OP_BF16>(stages, n, done, status, trace, num_sms, s);
+    case OP_I8: return launch_chain_op<OP_I8>(stages, n, done, status, trace, num_sms, s);
     default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launch_tc_chain(const StageArgs *stages, int n, int *done, int *status,
-                            unsigned long long *trace, int num_sms, cudaStream_t s)
+// Many stages with their tables in device memory.
+template <int OP>
+static cudaError_t plan_pair_op(const StageArgs *stages, const int *prev, int n, int num_sms,
+                                GroupLaunch &out)
 {
-    std::vector<int> prev(n);
-    for (int i = 0; i < n; ++i) prev[i] = i - 1;
-    return launch_tc_group(stages, prev.data(), n, done, status, trace, nullptr, num_sms, s);
+    using G = PairGeo<OP>;
+    std::vector<ChainStage> st(n);
+    long items = 0;
+    int done_off = 0;
+    for (int i = 0; i < n; ++i) {
+        if (prev[i] >= i) return cudaErrorInvalidValue;
+        cudaError_t e = make_chain_stage<OP>(stages[i], prev[i], done_off, st[i]);
+        if (e != cudaSuccess) return e;
+        done_off += st[i].tiles_n;
+        items += (long)st[i].tiles_m * st[i].tiles_n;
+    }
+    int pairs = 0;
+    cudaError_t e = pair_capacity<OP>(num_sms, pairs);
+    if (e != cudaSuccess) return e;
+    if (items < pairs) pairs = (int)items;
+    std::vector<int> off;
+    std::vector<WorkEntry> ent;
+    const std::vector<SchedStage> ss = sched_stages(st, G::BK);
+    list_schedule(ss.data(), n, pairs, 2.0, off, ent);
+    auto r = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    out.kernel = GK_PAIR;
+    out.op = OP;
+    out.ctas = 2 * pairs;
+    out.entries = items;
+    out.done_ints = (size_t)done_off;
+    out.off_st = 0;
+    out.off_sched = r((size_t)n * sizeof(ChainStage));
+    out.off_off = out.off_sched + r((size_t)items * sizeof(WorkEntry));
+    out.tables.assign(out.off_off + r((size_t)(pairs + 1) * sizeof(int)), 0);
+    memcpy(out.tables.data(), st.data(), (size_t)n * sizeof(ChainStage));
+    memcpy(out.tables.data() + out.off_sched, ent.data(), (size_t)items * sizeof(WorkEntry));
+    memcpy(out.tables.data() + out.off_off, off.data(), (size_t)(pairs + 1) * sizeof(int));
+    return cudaSuccess;
+}
+
+cudaError_t plan_pair_group(const StageArgs *stages, const int *prev, int n, int num_sms,
+                            GroupLaunch &out)
+{
+    if (n < 1) return cudaErrorInvalidValue;
+    for (int i = 0; i < n; ++i)
+        if (stages[i].op != stages[0].op || stages[i].M <= 0 || stages[i].K <= 0 ||
+            stages[i].N <= 0)
+            return cudaErrorInvalidValue;
+    switch (stages[0].op) {
+    case OP_BF16: return plan_pair_op<OP_BF16>(stages, prev, n, num_sms, out);
+    case OP_I8: return plan_pair_op<OP_I8>(stages, prev, n, num_sms, out);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_pair_group(const GroupLaunch &g, const void *tables_dev, int *done,
+                              int *status, cudaStream_t s)
+{
+    static thread_local ChainParams P;  // only the device-table fields are used
+    P.ext_st = reinterpret_cast<const ChainStage *>(static_cast<const unsigned char *>(tables_dev) +
+                                                    g.off_st);
+    P.ext_sched = reinterpret_cast<const WorkEntry *>(
+        static_cast<const unsigned char *>(tables_dev) + g.off_sched);
+    P.ext_off = reinterpret_cast<const int *>(static_cast<const unsigned char *>(tables_dev) +
+                                              g.off_off);
+    P.npairs = g.ctas / 2;
+    P.done = done;
+    P.status = status;
+    P.trace = nullptr;
+    switch (g.op) {
+    case OP_BF16: return launch_pairs<OP_BF16, true>(P, g.ctas / 2, s);
+    case OP_I8: return launch_pairs<OP_I8, true>(P, g.ctas / 2, s);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 int chain_max_stages() { return kChainMaxStages; }

@@ -22,23 +22,20 @@
 
 namespace fg {
 
+// One BM x BN output tile at (m0, n0); As / Bs are the block's double buffers.
 template <int BM, int BN, int BK, int TM, int TN, bool VEC, bool KSPLIT>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN))
-    ffma_sgemm_kernel(const FfmaArgs p)
+__device__ __forceinline__ void ffma_tile(const FfmaArgs &p, int m0, int n0,
+                                          float (*As)[BK][BM], float (*Bs)[BK][BN])
 {
     constexpr int NT = (BM / TM) * (BN / TN);
     constexpr int A_LOADS = BM * BK / NT;  // elements per thread per slice
     constexpr int B_LOADS = BK * BN / NT;
     static_assert(A_LOADS % 4 == 0 && B_LOADS % 4 == 0, "vector tiling");
     static_assert(TM % 4 == 0 && TN % 4 == 0, "float4 fragments");
-    __shared__ __align__(16) float As[2][BK][BM];
-    __shared__ __align__(16) float Bs[2][BK][BN];
 
     const int tid = threadIdx.x;
     const int tx = tid % (BN / TN);
     const int ty = tid / (BN / TN);
-    const int m0 = blockIdx.y * BM;
-    const int n0 = blockIdx.x * BN;
     const int M = p.M, N = p.N, K = p.K;
 
     // A: a thread loads A_LOADS consecutive k of one row; B: B_LOADS consecutive n of one k row.
@@ -207,6 +204,59 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
             }
         }
     }
+}
+
+template <int BM, int BN, int BK, int TM, int TN, bool VEC, bool KSPLIT>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+    ffma_sgemm_kernel(const FfmaArgs p)
+{
+    __shared__ __align__(16) float As[2][BK][BM];
+    __shared__ __align__(16) float Bs[2][BK][BN];
+    ffma_tile<BM, BN, BK, TM, TN, VEC, KSPLIT>(p, blockIdx.y * BM, blockIdx.x * BN, As, Bs);
+}
+
+// Many independent SGEMMs: CTA b works on job j with tile0[j] <= b < tile0[j + 1].
+template <int BM, int BN, int BK, int TM, int TN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+    ffma_group_kernel(const FfmaJob *__restrict__ jobs, int njobs)
+{
+    __shared__ __align__(16) float As[2][BK][BM];
+    __shared__ __align__(16) float Bs[2][BK][BN];
+    const int b = blockIdx.x;
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].tile0 <= b)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const FfmaJob &j = jobs[lo];
+    const int t = b - j.tile0;
+    FfmaArgs p;
+    p.M = j.M; p.N = j.N; p.K = j.K;
+    p.A = j.A; p.lda = j.lda;
+    p.B = j.B; p.ldb = j.ldb;
+    p.C = j.C; p.ldc = j.ldc;
+    p.kblock = 0;
+    const int m0 = (t / j.tiles_n) * BM, n0 = (t % j.tiles_n) * BN;
+    if (j.vec)
+        ffma_tile<BM, BN, BK, TM, TN, true, false>(p, m0, n0, As, Bs);
+    else
+        ffma_tile<BM, BN, BK, TM, TN, false, false>(p, m0, n0, As, Bs);
+}
+
+int ffma_group_tile(int big) { return big ? 128 : 64; }
+
+cudaError_t launch_ffma_group(const FfmaJob *jobs_dev, int njobs, int total_tiles, int big,
+                              cudaStream_t s)
+{
+    if (njobs < 1 || total_tiles < 1) return cudaSuccess;
+    if (big)
+        ffma_group_kernel<128, 128, 16, 8, 8><<<total_tiles, 256, 0, s>>>(jobs_dev, njobs);
+    else
+        ffma_group_kernel<64, 64, 16, 4, 8><<<total_tiles, 128, 0, s>>>(jobs_dev, njobs);
+    return cudaGetLastError();
 }
 
 template <int BM, int BN, int BK, int TM, int TN>

@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <vector>
+
 namespace fg {
 
 // How a tensor-core GEMM stage writes its result.
@@ -57,15 +59,72 @@ cudaError_t launch_tc_chain(const StageArgs *stages, int n, int *done, int *stat
 int chain_max_stages();
 int chain_trace_fields();
 
-// Several chains of one op in one launch: stage i reads the output of stage
-// prev[i] (-1: a chain's first stage; prev[i] < i). `done` holds
-// sum_i ceil(N_i / 256) zeroed ints; ext_dev (device memory of
-// chain_group_table_bytes(n, work entries) bytes, or null) holds the stage table
-// and schedule when they do not fit in the kernel parameters.
-cudaError_t launch_tc_group(const StageArgs *stages, const int *prev, int n, int *done,
-                            int *status, unsigned long long *trace, void *ext_dev, int num_sms,
-                            cudaStream_t s);
-size_t chain_group_table_bytes(int nstages, long items);
+// ------------------------------------------------------------------ grouped launches
+//
+// Many chains' stages in one persistent launch. Stage i reads the output of
+// stage prev[i] (-1: a chain's first stage; prev[i] < i). Every worker (a CTA,
+// or a CTA pair) runs its own list of tiles in order; a tile first waits until
+// all tiles of the column block it reads are stored (a counter per column block
+// of each stage, released by the epilogue warps).
+
+// One tile: stage index and (row block << 16 | column block).
+struct WorkEntry {
+    uint32_t stage;
+    uint32_t mbnb;
+};
+
+struct SchedStage {
+    int tiles_m, tiles_n;  // tiles of the stage along M and N
+    int prev;              // stage it reads (-1: none), earlier in the list
+    int done_off;          // its first column-block counter
+    double cost;           // estimated duration of one tile (any unit)
+};
+
+// List schedule: stages in dependency depth order, each stage's tiles column
+// block by column block; a tile goes to the worker that can start it first (the
+// worker is free and the column block it reads is estimated done + handoff).
+// Worker u runs entries[off[u] .. off[u+1]) in that order, so the earliest
+// unfinished entry always heads its worker's list and no worker waits forever.
+// makespan (optional): the estimated finish time of the last tile.
+void list_schedule(const SchedStage *st, int n, int units, double handoff, std::vector<int> &off,
+                   std::vector<WorkEntry> &entries, double *makespan = nullptr);
+
+enum GroupKernel : int {
+    GK_PAIR = 0,        // BF16 / INT8: CTA pairs, 256 x 256 tiles, 6-stage ring
+    GK_SINGLE_256 = 1,  // BF16 / INT8: single CTAs, 128 x 256 tiles, 4-stage ring
+    GK_SINGLE_128 = 2,  // BF16 / INT8: single CTAs, 128 x 128 tiles, 6-stage ring;
+                        // 3xTF32: 128 x 128 tiles, 3-stage ring (its only kernel)
+};
+
+// A planned grouped launch: device tables (copied to device memory as they are,
+// at a 256-byte-aligned address) and the launch shape.
+struct GroupLaunch {
+    int kernel = GK_PAIR;
+    int op = 0;
+    int ctas = 0;             // CTAs launched (pairs x 2 for GK_PAIR)
+    long entries = 0;         // tiles
+    size_t done_ints = 0;     // zeroed counters the launch needs
+    size_t off_st = 0, off_sched = 0, off_off = 0;  // table offsets in `tables`
+    std::vector<unsigned char> tables;
+};
+
+// Column width of a kernel's tiles (the unit of its dependency counters).
+int group_tile_n(int kernel, int op);
+cudaError_t plan_group(const StageArgs *stages, const int *prev, int n, int kernel, int num_sms,
+                       GroupLaunch &out);
+cudaError_t launch_group(const GroupLaunch &g, const void *tables_dev, int *done, int *status,
+                         cudaStream_t s);
+
+// Pair-kernel pieces behind plan_group / launch_group (fg_chain_fused.cu) and
+// the single-CTA ones (fg_group.cu).
+cudaError_t plan_pair_group(const StageArgs *stages, const int *prev, int n, int num_sms,
+                            GroupLaunch &out);
+cudaError_t launch_pair_group(const GroupLaunch &g, const void *tables_dev, int *done,
+                              int *status, cudaStream_t s);
+cudaError_t plan_single_group(const StageArgs *stages, const int *prev, int n, int kernel,
+                              int num_sms, GroupLaunch &out);
+cudaError_t launch_single_group(const GroupLaunch &g, const void *tables_dev, int *done,
+                                int *status, cudaStream_t s);
 
 // Plain FP32 SGEMM on CUDA cores: C = A * B, one FMA per k in increasing k;
 // with kblock > 0 each block of kblock k is summed from zero and added to C.
@@ -88,6 +147,31 @@ cudaError_t launch_split_tf32(const float *in, long ld_in, float *hi, float *lo,
 cudaError_t launch_prep_int8_weights(const int8_t *src, long ld_in, uint8_t *dst, long ld_out,
                                      long M, long K, long tail_lo, long tail_hi,
                                      cudaStream_t s);
+
+// FP32 -> (hi, lo) TF32 splits of many matrices in one launch (jobs in device memory).
+struct SplitJob {
+    const float *in;
+    long ld_in;
+    float *hi, *lo;
+    long ld_out, rows, cols;
+};
+cudaError_t launch_split_tf32_jobs(const SplitJob *jobs_dev, int njobs, long max_elems,
+                                   cudaStream_t s);
+
+// Plain FP32 SGEMMs of many independent jobs in one launch (jobs in device
+// memory; job j owns CTAs [tile0[j], tile0[j + 1]) ).
+struct FfmaJob {
+    int M, N, K;
+    const float *A; long lda;
+    const float *B; long ldb;
+    float *C; long ldc;
+    int tile0;   // first CTA of this job
+    int tiles_n; // column tiles of this job
+    int vec;     // 16-byte-aligned rows and pointers
+};
+int ffma_group_tile(int big);  // tile edge of the grouped FFMA kernel (64, or 128 when big)
+cudaError_t launch_ffma_group(const FfmaJob *jobs_dev, int njobs, int total_tiles, int big,
+                              cudaStream_t s);
 
 // The same preparation for up to 8 matrices in one launch.
 struct PrepJob {

@@ -118,13 +118,66 @@ typedef struct {
     const fg_weights *W;
 } fg_chain_desc;
 
-/* Many independent chains of one dtype in ONE persistent launch (BF16, INT8):
- * the CTA pairs of the grid walk all chains' tiles together under a schedule
- * the host computes per shape set (cached), each chain's stages ordered by
- * their per-block completion counters. Chains of uneven lengths and shapes mix
- * freely. FP32 chains (no grouped FP32 kernel) run one after another.
- * Asynchronous, ordered on `stream` like fg_chain_dev. */
+/* Many independent chains of one dtype in one grouped launch. BF16 / INT8 /
+ * FP32-3xTF32: one persistent tensor-core kernel; every CTA (or CTA pair) of
+ * the grid walks its share of all chains' tiles under a schedule the host
+ * computes per shape set, and a tile of a chain's next stage starts as soon as
+ * the column block it reads is complete. FP32 with FG_F32_FFMA: one grouped
+ * CUDA-core launch per chain depth. Chains of uneven lengths and shapes mix
+ * freely; results are bit-identical to running each chain alone with the same
+ * kernel choice. The kernel and stage order come from fg_set_group_config (by
+ * default the autotuner's choice). Asynchronous, ordered on `stream` like
+ * fg_chain_dev. Corresponds to no reference entry point (the reference runs
+ * one chain per call, multigemm/src/flashgemm.c:46). */
 int fg_chain_group(int dtype, int nchains, const fg_chain_desc *chains, void *stream);
+
+/* Kernel of a grouped launch. */
+enum {
+    FG_GROUP_AUTO = -1,      /* autotuned: measured choice for the shape set, else the cost model */
+    FG_GROUP_PAIR = 0,       /* BF16 / INT8: CTA pairs (cta_group::2), 256 x 256 tiles, 6-stage ring */
+    FG_GROUP_SINGLE_256 = 1, /* BF16 / INT8: single CTAs, 128 x 256 tiles, 4-stage ring */
+    FG_GROUP_SINGLE_128 = 2  /* BF16 / INT8: single CTAs, 128 x 128 tiles, 6-stage ring;
+                                FP32 3xTF32: 128 x 128 tiles, 3-stage ring (its only kernel) */
+};
+/* Stage order of a grouped launch. */
+enum {
+    FG_ORDER_AUTO = -1,
+    FG_ORDER_FUSED = 0,  /* one launch; intermediates handed over per column block through L2 */
+    FG_ORDER_LEVELS = 1  /* one launch per chain depth; each level spills its outputs to HBM */
+};
+/* Process-wide choice for later groups and plans (FG_GROUP_AUTO / FG_ORDER_AUTO:
+ * the autotuner decides). */
+void fg_set_group_config(int kernel, int order);
+void fg_get_group_config(int *kernel, int *order);
+
+/* A planned grouped launch, bound to its chains' buffers: tables, schedule and
+ * intermediate buffers are built and uploaded once, so a launch is kernel
+ * launches only and can be captured in a CUDA graph. */
+typedef struct fg_plan_s *fg_plan;
+int fg_plan_create(int dtype, int nchains, const fg_chain_desc *chains, fg_plan *out);
+/* Stream-ordered launches of the plan on `stream` (NULL: legacy default stream). */
+int fg_plan_launch(fg_plan plan, void *stream);
+/* The first call captures fg_plan_launch into a CUDA graph; every call
+ * launches that graph on `stream` (one launch for the whole group). */
+int fg_plan_launch_graph(fg_plan plan, void *stream);
+/* The plan's kernel and order (resolved), device bytes it owns, kernels per
+ * launch, and total GEMM FLOPs. Any pointer may be NULL. */
+int fg_plan_info(fg_plan plan, int *kernel, int *order, long *device_bytes, int *kernels,
+                 double *flops);
+/* Waits for the device to be idle, then frees the plan. */
+int fg_plan_release(fg_plan plan);
+
+/* Autotuner: times every (kernel, order) candidate on this group (`iters` timed
+ * launches each after one warm-up, CUDA events on a private stream, buffers
+ * overwritten) and remembers the fastest for the group's shape signature,
+ * which FG_GROUP_AUTO groups of the same shapes then use. Outputs may be NULL. */
+int fg_autotune_group(int dtype, int nchains, const fg_chain_desc *chains, int iters,
+                      int *kernel, int *order, double *best_ms);
+/* Remembered choices to / from a text file (one line per shape signature). */
+int fg_autotune_save(const char *path);
+int fg_autotune_load(const char *path);
+/* Choice for a group without measuring (remembered, else the cost model). */
+int fg_group_choice(int dtype, int nchains, const fg_chain_desc *chains, int *kernel, int *order);
 
 /* Wait for all of the library's work on the current device and report any
  * kernel-side error since the last fg_sync (then cleared). */
