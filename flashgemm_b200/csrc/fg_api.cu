@@ -918,6 +918,15 @@ int register_weights(int dtype, const void *A, long M, long K, int where, fg_wei
         return FG_OK;
     };
     const size_t main_bytes = (size_t)M * w->ld * elt;
+    if (where == FG_MEM_DEVICE) {
+        // the source may still be written by work on any stream: registration is
+        // a one-time step, so it waits for the device to be idle
+        cudaError_t e0 = cudaDeviceSynchronize();
+        if (e0 != cudaSuccess) {
+            delete w;
+            return fail(FG_ERR_CUDA, "weights: %s", cudaGetErrorString(e0));
+        }
+    }
     if ((st = alloc(&w->main, main_bytes))) {
         free_weights(w);
         return st;

@@ -94,7 +94,9 @@ int fg_sgemm_dev(float *C, const float *A, const float *B, long M, long N, long 
  * (FP32: the 3xTF32 hi/lo split; INT8: the reference's shifted tail-row
  * block), so chains on them skip every per-call weight preparation. A is
  * M x K row-major (leading dimension K) in host (FG_MEM_HOST) or device
- * (FG_MEM_DEVICE) memory. Blocking. */
+ * (FG_MEM_DEVICE) memory; a device source is read after the device is idle
+ * (cudaDeviceSynchronize), so work on any stream that writes it is complete.
+ * Blocking. */
 typedef struct fg_weights_s *fg_weights;
 enum { FG_MEM_HOST = 0, FG_MEM_DEVICE = 1 };
 int fg_weights_register(int dtype, const void *A, long M, long K, int where, fg_weights *out);
