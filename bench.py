@@ -1,7 +1,7 @@
 """Benchmark of the flashgemm hot path on B200: one JSON line on stdout.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload bf16-chain|int8-chain|f32-gemm]
+                    [--workload bf16-chain|int8-chain|f32-gemm|bf16-gemm|int8-gemm|f32-groups]
 
 A step is one pass of the hot path over one batch: by default the BF16 chain
 of three GEMMs C = A3*(A2*(A1*B)) with B 1024 x 4096 (the activations X
@@ -20,6 +20,13 @@ max-over-ranks time.
 its sources into oracle/_ref) on this machine's host cores, on a bounded
 column sample of the same workload, and prints the same line with
 "impl": "reference".
+
+--workload f32-groups: 512 independent FP32 chains (length 2-5, dimensions
+log-uniform on multiples of 16 in [64, 4096], activation columns up to 8192,
+plus tall-skinny chains of 65536 columns with 64 x 64 weights), N(0,1)/sqrt(K)
+entries, run as one graph-captured grouped 3xTF32 launch; the same group
+through the plain FP32 kernel beside it, and both errors against FP64 on a
+seeded sample of the chains.
 """
 import argparse
 import json
@@ -248,22 +255,343 @@ def make_inputs(dt, N, K1, Ms, seed):
     return B, As, Ks
 
 
+# ---------------------------------------------------------------- grouped FP32 chains
+
+GROUP_CHAINS = 512
+GROUP_SKINNY = 8
+
+
+def group_specs(seed, count=GROUP_CHAINS, skinny=GROUP_SKINNY):
+    """(N, K1, [M_1..M_n]) of the grouped workload: chain length U{2..5},
+    dimensions log-uniform on multiples of 16 in [64, 4096], activation columns
+    log-uniform in [64, 8192], plus `skinny` chains of 65536 columns with 64 x 64
+    weights; shuffled."""
+    rng = np.random.default_rng(seed)
+
+    def dim(lo, hi):
+        v = int(16 * round(float(np.exp(rng.uniform(np.log(lo), np.log(hi)))) / 16))
+        return min(max(v, lo), hi)
+
+    specs = []
+    for _ in range(count - skinny):
+        n = int(rng.integers(2, 6))
+        N = dim(64, 8192)
+        dims = [dim(64, 4096) for _ in range(n + 1)]
+        specs.append((N, dims[0], dims[1:]))
+    for _ in range(skinny):
+        n = int(rng.integers(2, 6))
+        specs.append((65536, 64, [64] * n))
+    order = rng.permutation(len(specs))
+    return [specs[i] for i in order]
+
+
+def group_sample(specs, seed, count=16, skinny=2, max_gflop=20.0):
+    """Indices of the chains checked against FP64 and timed on the CPU."""
+    rng = np.random.default_rng(seed)
+    small = [i for i, (N, K1, Ms) in enumerate(specs)
+             if N != 65536 and flops_of(N, K1, Ms) <= max_gflop * 1e9]
+    thin = [i for i, (N, _, _) in enumerate(specs) if N == 65536]
+    pick = list(rng.choice(small, size=min(count, len(small)), replace=False))
+    return sorted(int(i) for i in pick + thin[:skinny])
+
+
+def group_cpu(specs, sample, host, steps=None, budget_s=12.0):
+    """The reference's FP32 chain (or the C port) on the sampled chains, all
+    host threads: TFLOP/s over the sample. steps=None: repeat for budget_s."""
+    oracle, kind, model, amx = reference_runner()
+    threads = os.cpu_count() or 1
+    fl = sum(flops_of(*specs[i]) for i in sample)
+
+    def one():
+        for i in sample:
+            N, K1, Ms = specs[i]
+            B, As = host[i]
+            Ks = [K1] + Ms[:-1]
+            if kind == "reference":
+                oracle.ref_chain("f32", B, As, N, Ms, Ks, threads=threads)
+            else:
+                oracle.chain("f32", B, As, N, Ms, Ks)
+    one()
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while True:
+        t0 = time.perf_counter()
+        one()
+        times.append(time.perf_counter() - t0)
+        if steps is not None:
+            if len(times) >= steps:
+                break
+        elif len(times) >= 3 and time.perf_counter() > t_end:
+            break
+    med = statistics.median(times)
+    descr = {"kind": kind, "cores": threads, "cpu": model, "amx_available": amx,
+             "amx_used": False,
+             "sample": f"{len(sample)} of the group's {len(specs)} chains "
+                       f"({fl / 1e9:.1f} GFLOP per step, all of each chain), median of "
+                       f"{len(times)} steps"}
+    return fl / med / 1e12, descr, times
+
+
+def group_host_inputs(specs, indices, seed):
+    """Host operands (B, [A_i]) of chosen chains with the workload's
+    distributions, drawn on the host (chain j from seed + j): inputs for timing
+    the CPU reference where no GPU drew them."""
+    import torch
+    out = {}
+    for j in indices:
+        N, K1, Ms = specs[j]
+        g = torch.Generator().manual_seed(seed + j)
+        Ks = [K1] + Ms[:-1]
+        As = [(torch.randn(m, k, generator=g) / float(np.sqrt(k))).numpy() for m, k in zip(Ms, Ks)]
+        B = torch.randn(K1, N, generator=g).numpy()
+        out[j] = (np.ascontiguousarray(B), [np.ascontiguousarray(a) for a in As])
+    return out
+
+
+def run_groups(args, world, rank, local_rank):
+    seed = 4321
+    specs = group_specs(seed)
+    sample = group_sample(specs, seed + 1)
+    total_flops = sum(flops_of(*s) for s in specs)
+    config = {"workload": "512 independent FP32 chains in one graph-captured grouped launch: "
+                          "length U{2..5}, dims log-uniform on multiples of 16 in [64, 4096], "
+                          "activation columns log-uniform in [64, 8192], 8 tall-skinny chains "
+                          "(65536 columns, 64 x 64 weights); N(0,1)/sqrt(K) entries",
+              "chains": len(specs), "stages": sum(len(s[2]) for s in specs),
+              "gflop_per_step_per_gpu": total_flops / 1e9,
+              "l2": "flushed between steps (256 MiB write outside the step events)",
+              "parallelism": f"dp{world} (each rank runs its own group, no collective)"}
+    metric = "grouped FP32 chains TFLOP/s (3xTF32)"
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        host = group_host_inputs(specs, sample, seed)
+        tf, descr, times = group_cpu(specs, sample, host, steps=args.steps)
+        line = {"impl": "reference", "metric": metric, "value": tf, "unit": "TFLOP/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * statistics.median(times), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded)", "config": config,
+                "cpu_baseline": dict(descr, value=tf, unit="TFLOP/s"),
+                "e2e": {"value": tf, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    import flashgemm_b200 as fg
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+    fg.lib()
+    # operands: weights registered once (resident), activations and outputs in HBM;
+    # chain j draws from seed + j (+ rank offset), on the device
+    chains = []
+    host = {}  # the sampled chains' operands, copied back for the FP64 check
+    t_gen = time.perf_counter()
+    for j, (N, K1, Ms) in enumerate(specs):
+        g = torch.Generator(device=dev).manual_seed(seed + j + 100000 * rank)
+        Ks = [K1] + Ms[:-1]
+        W, keep = [], []
+        for m, k in zip(Ms, Ks):
+            a = torch.randn(m, k, generator=g, device=dev) / float(np.sqrt(k))
+            W.append(fg.Weights("f32", a))
+            if j in sample:
+                keep.append(a.cpu().numpy())
+            del a
+        B = torch.randn(K1, N, generator=g, device=dev)
+        if j in sample:
+            host[j] = (B.cpu().numpy(), keep)
+        C = torch.empty(Ms[-1], N, device=dev)
+        chains.append((C, B, N, W))
+    t_gen = time.perf_counter() - t_gen
+    weight_bytes = sum(w.nbytes for c in chains for w in c[3])
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def timed(plan, sampler=None):
+        for _ in range(max(args.warmup, 3)):
+            plan.launch(graph=True)
+        torch.cuda.synchronize(dev)
+        fg.sync()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        l0 = fg.kernel_launches()
+        with (sampler if sampler is not None else _Null()):
+            for i in range(args.steps):
+                flush.fill_(i & 0xFF)
+                starts[i].record()
+                plan.launch(graph=True)
+                stops[i].record()
+            torch.cuda.synchronize(dev)
+        fg.sync()
+        launches = fg.kernel_launches() - l0
+        ms = sum(a.elapsed_time(b) for a, b in zip(starts, stops))
+        if dist:
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, launches
+
+    def kernel_profile(plan, kind, n=5):
+        """Average device time of the plan's main kernel, CUDA events on the
+        stream it runs on (direct launches; a graph replay runs the same kernels)."""
+        fg.profile_begin()
+        for _ in range(n):
+            flush.fill_(1)
+            plan.launch(graph=False)
+        torch.cuda.synchronize(dev)
+        fg.sync()
+        fg.profile_end()
+        return fg.profile_query(kind)
+
+    def sample_out():
+        return {j: chains[j][0].cpu().numpy().copy() for j in sample}
+
+    # ---- 3xTF32: autotuned stage order, one graph-captured launch per step
+    fg.set_f32_algo("3xtf32")
+    tune = fg.autotune_group("f32", chains, iters=2)
+    plan = fg.Plan("f32", chains)
+    info = plan.info()
+    sampler = ClockSampler(torch.cuda.current_device())
+    x3_ms, launches = timed(plan, sampler)
+    k_ms, k_n, k_fl = kernel_profile(plan, fg.FG_PK_TC_TF32X3)
+    out_x3 = sample_out()
+
+    # ---- end to end: host activations in, host results out, every step
+    e2e_steps = args.e2e_steps or 3
+    hB = [torch.empty(tuple(c[1].shape), dtype=torch.float32, pin_memory=True) for c in chains]
+    hC = [torch.empty(tuple(c[0].shape), dtype=torch.float32, pin_memory=True) for c in chains]
+    for h, c in zip(hB, chains):
+        h.copy_(c[1])
+
+    def e2e_step():
+        for h, c in zip(hB, chains):
+            c[1].copy_(h, non_blocking=True)
+        plan.launch(graph=True)
+        for h, c in zip(hC, chains):
+            h.copy_(c[0], non_blocking=True)
+        torch.cuda.synchronize(dev)
+
+    e2e_step()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = sum(h.numel() * 4 for h in hB)
+    d2h = sum(h.numel() * 4 for h in hC)
+    del hB, hC
+    plan.release()
+
+    # ---- plain FP32 (FFMA, one grouped launch per chain depth)
+    fg.set_f32_algo("ffma")
+    plan2 = fg.Plan("f32", chains)
+    ff_ms, _ = timed(plan2)
+    out_ff = sample_out()
+    plan2.release()
+    fg.set_f32_algo("3xtf32")
+    for c in chains:
+        for w in c[3]:
+            w.release()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    # ---- accuracy against FP64 on the sample (host)
+    err_x3, err_ff = [], []
+    for j in sample:
+        B, As = host[j]
+        exact = B.astype(np.float64)
+        for a in As:
+            exact = a.astype(np.float64) @ exact
+        nrm = np.linalg.norm(exact)
+        err_x3.append(float(np.linalg.norm(out_x3[j] - exact) / nrm))
+        err_ff.append(float(np.linalg.norm(out_ff[j] - exact) / nrm))
+    ratio = [a / b for a, b in zip(err_x3, err_ff) if b > 0]
+
+    value = world * total_flops * args.steps / (x3_ms / 1e3) / 1e12
+    plain = world * total_flops * args.steps / (ff_ms / 1e3) / 1e12
+    peaks, peak_src = load_peaks()
+    peak = peaks.get("bf16_tflops") / 2.0 / 3.0
+    achieved = k_fl / (k_ms / 1e3) / 1e12 if k_ms > 0 else None
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak if achieved else None, "traffic": None,
+                "kernel": "fg::tc_group_kernel<OP_TF32X3,128,3> (all chains, one launch per order level)",
+                "launches_timed": k_n, "avg_launch_us": 1e3 * k_ms / k_n if k_n else None,
+                "peak_source": "bf16_tflops / 2 (dense TF32 is half the BF16 rate) / 3 "
+                               f"(three MMAs per 3xTF32 product); {peak_src}"}
+    names = {0: "fused", 1: "levels"}
+    line = {"metric": metric, "value": value, "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": x3_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (3xTF32 split on tensor cores, FP32 accumulate)",
+            "data": "synthetic (seeded; no dataset involved)", "config": config,
+            "clocks": sampler.summary(), "gpu_launches": launches,
+            "e2e": {"value": world * total_flops * e2e_steps / e2e_s / 1e12, "unit": "TFLOP/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                    "api": "fg_plan_launch_graph on registered weights; every chain's B copied "
+                           "from pinned host memory and C copied back each step"},
+            "roofline": roofline,
+            "plain_fp32": {"value": plain, "unit": "TFLOP/s", "ms_per_step": ff_ms / args.steps,
+                           "path": "grouped FFMA kernel, one launch per chain depth"},
+            "x3_vs_plain": value / plain,
+            "accuracy": {"sample_chains": len(sample),
+                         "rel_frob_vs_fp64_3xtf32_max": max(err_x3),
+                         "rel_frob_vs_fp64_plain_max": max(err_ff),
+                         "ratio_3xtf32_over_plain_max": max(ratio) if ratio else None},
+            "plan": {"order": names.get(info["order"], info["order"]),
+                     "autotune": {"order": names.get(tune[1], tune[1]), "ms": tune[2]},
+                     "device_bytes": info["device_bytes"], "kernels_per_step": info["kernels"],
+                     "weight_bytes": weight_bytes, "setup_s": t_gen}}
+    if world == 1:
+        tf, descr, _ = group_cpu(specs, sample, host, budget_s=args.cpu_budget)
+        line["cpu_baseline"] = dict(descr, value=tf, unit="TFLOP/s")
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 1000; f32-groups 20)")
+    ap.add_argument("--warmup", type=int, default=None,
+                    help="untimed steps (default 20; f32-groups 3)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="bf16-chain", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="bf16-chain",
+                    choices=list(WORKLOADS) + ["f32-groups"])
     ap.add_argument("--e2e-steps", type=int, default=None,
                     help="steps of the host-buffer C-ABI measurement (default: min(steps, 200))")
     ap.add_argument("--cpu-budget", type=float, default=12.0,
                     help="seconds of reference CPU work for the cpu_baseline leg")
     args = ap.parse_args()
+    grouped = args.workload == "f32-groups"
+    if args.steps is None:
+        args.steps = 20 if grouped else 1000
+    if args.warmup is None:
+        args.warmup = 3 if grouped else 20
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if grouped:
+        return run_groups(args, world, rank, local_rank)
     dt, N, K1, Ms = WORKLOADS[args.workload]
     metric = {"f32": "FP32 GEMM TFLOP/s"}.get(dt, "fused GEMM-chain TFLOP/s")
     config = {"workload": DESCR[args.workload], "dtype": dt, "N": N, "K1": K1, "M": Ms,

@@ -457,3 +457,102 @@ class Plan:
             self.release()
         except Exception:  # noqa: BLE001 - interpreter shutdown
             pass
+
+
+# ---------------------------------------------------------------- serving loop
+
+class _Request(ctypes.Structure):
+    _fields_ = [("dtype", ctypes.c_int), ("num_gemm", ctypes.c_int), ("W", _P), ("N", _L),
+                ("B", _P), ("C", _P), ("where", ctypes.c_int)]
+
+
+class _ServerOpts(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_longlong), ("max_batch", ctypes.c_int),
+                ("slots", ctypes.c_int), ("max_wait_us", ctypes.c_int),
+                ("ctas_per_batch", ctypes.c_int)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+                ("failed", ctypes.c_longlong), ("batches", ctypes.c_longlong),
+                ("mean_batch", ctypes.c_double), ("p50_us", ctypes.c_double),
+                ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double),
+                ("max_us", ctypes.c_double), ("flops", ctypes.c_double),
+                ("span_s", ctypes.c_double), ("peak_bytes", ctypes.c_longlong)]
+
+
+class Server:
+    """The library's request loop (fg_server_*): chain requests on registered
+    weights, admitted by device memory, batched into grouped launches."""
+
+    def __init__(self, hbm_budget=0, max_batch=0, slots=0, max_wait_us=0, ctas_per_batch=0):
+        L = lib()
+        L.fg_server_create.argtypes = [_P, _P]
+        L.fg_server_submit.argtypes = [_P, _P]
+        L.fg_server_submit.restype = ctypes.c_longlong
+        L.fg_server_wait.argtypes = [_P, ctypes.c_longlong, _P]
+        L.fg_server_drain.argtypes = [_P]
+        L.fg_server_get_stats.argtypes = [_P, _P]
+        L.fg_server_reset_stats.argtypes = [_P]
+        L.fg_server_destroy.argtypes = [_P]
+        o = _ServerOpts(int(hbm_budget), int(max_batch), int(slots), int(max_wait_us),
+                        int(ctas_per_batch))
+        h = _P()
+        st = L.fg_server_create(ctypes.byref(o), ctypes.byref(h))
+        if st != FG_OK:
+            raise FlashgemmError(st, last_error())
+        self.handle = h.value
+        self._keep = {}
+
+    def submit(self, dtype, weights, B, C, N=None):
+        """Queue C = A_n ... A_1 B on `weights` (list of Weights). B and C are
+        host numpy arrays or CUDA tensors (both the same kind); returns the id."""
+        L = lib()
+        host = isinstance(B, np.ndarray)
+        N = int(B.shape[1] if N is None else N)
+        hs = (_P * len(weights))(*[w.handle for w in weights])
+        ptr = (lambda a: a.ctypes.data) if host else (lambda a: a.data_ptr())
+        r = _Request(_DT[dtype], len(weights), ctypes.cast(hs, _P), N, ptr(B), ptr(C),
+                     FG_MEM_HOST if host else FG_MEM_DEVICE)
+        rid = L.fg_server_submit(self.handle, ctypes.byref(r))
+        if rid < 0:
+            raise FlashgemmError(-rid, last_error())
+        self._keep[rid] = (hs, B, C, weights)
+        return rid
+
+    def wait(self, rid):
+        """Blocks until request `rid` is done; returns its latency in microseconds."""
+        L = lib()
+        lat = ctypes.c_double()
+        st = L.fg_server_wait(self.handle, ctypes.c_longlong(rid), ctypes.byref(lat))
+        self._keep.pop(rid, None)
+        if st != FG_OK:
+            raise FlashgemmError(st, last_error())
+        return lat.value
+
+    def drain(self):
+        st = lib().fg_server_drain(self.handle)
+        if st != FG_OK:
+            raise FlashgemmError(st, last_error())
+
+    def stats(self):
+        s = _ServerStats()
+        st = lib().fg_server_get_stats(self.handle, ctypes.byref(s))
+        if st != FG_OK:
+            raise FlashgemmError(st, last_error())
+        return {k: getattr(s, k) for k, _ in _ServerStats._fields_}
+
+    def reset_stats(self):
+        lib().fg_server_reset_stats(self.handle)
+
+    def close(self):
+        if self.handle:
+            lib().fg_server_destroy(self.handle)
+            self.handle = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass

@@ -434,7 +434,9 @@ cudaError_t pair_capacity(int num_sms, int &pairs)
         cfg.dynamicSmemBytes = G::SMEM_BYTES;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        cfg.gridDim = dim3(2 * (num_sms / 2));
+        int dev_sms = 0;
+        cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, dev);
+        cfg.gridDim = dim3(2 * (dev_sms / 2));
         int clusters = 0;
         e = cudaOccupancyMaxActiveClusters(&clusters, tc_chain_kernel<OP, false>, &cfg);
         if (e != cudaSuccess || clusters < 1) {
@@ -445,6 +447,7 @@ cudaError_t pair_capacity(int num_sms, int &pairs)
         known |= 1ull << (dev & 63);
     }
     pairs = cap[dev & 63];
+    if (pairs > num_sms / 2) pairs = num_sms / 2 > 0 ? num_sms / 2 : 1;  // a cap below the device
     return cudaSuccess;
 }
 

@@ -477,10 +477,10 @@ cudaError_t single_capacity(int num_sms, int &ctas)
             cudaGetLastError();
             return cudaErrorNotSupported;
         }
-        cap[dev & 63] = per_sm * num_sms;
+        cap[dev & 63] = per_sm;
         known |= 1ull << (dev & 63);
     }
-    ctas = cap[dev & 63];
+    ctas = cap[dev & 63] * num_sms;  // num_sms may be fewer than the device's: a cap
     return cudaSuccess;
 }
 

@@ -181,6 +181,66 @@ int fg_autotune_load(const char *path);
 /* Choice for a group without measuring (remembered, else the cost model). */
 int fg_group_choice(int dtype, int nchains, const fg_chain_desc *chains, int *kernel, int *order);
 
+/* ---------------------------------------------------------------- serving loop
+ *
+ * A request loop on the current device: chain requests on registered (resident)
+ * weights are admitted in arrival order while the device-memory budget and a
+ * launch slot allow, packed into grouped launches (one per dtype present) and
+ * run on one of `slots` streams, so a batch admitted while others are still on
+ * the GPU overlaps with them (each batch's persistent grid is capped at
+ * SMs / slots CTAs unless ctas_per_batch says otherwise). The device is never
+ * left idle while requests wait: a batch is launched at once when no other is
+ * in flight, else when it holds max_batch requests or its oldest request has
+ * waited max_wait_us. Results are the ones fg_chain_registered gives for the
+ * same request with the same kernel choice. The reference has no serving
+ * loop; this corresponds to none of its entry points. */
+typedef struct fg_server_s *fg_server;
+typedef struct {
+    long long hbm_budget;  /* device bytes for requests' activations, intermediates and
+                              tables (0: 80% of the free memory at creation) */
+    int max_batch;         /* requests per batch (0: 64) */
+    int slots;             /* batches in flight at once (0: 2) */
+    int max_wait_us;       /* batching window while the device is busy (0: 200) */
+    int ctas_per_batch;    /* grid cap of a batch's grouped kernels (0: SMs / slots) */
+} fg_server_opts;
+
+typedef struct {
+    int dtype;              /* FG_DT_*; FP32 runs with the current fg_get_f32_algo() */
+    int num_gemm;
+    const fg_weights *W;    /* registered weights, K_{i+1} = M_i (copied at submit) */
+    long N;                 /* activation columns; N * element size a multiple of 16 bytes */
+    const void *B;          /* K_0 x N row-major activations */
+    void *C;                /* M_{n-1} x N row-major result */
+    int where;              /* FG_MEM_HOST: B and C are host memory (copied in and out
+                               inside the request's latency; pinned memory copies
+                               asynchronously); FG_MEM_DEVICE: device memory, used in place */
+} fg_request;
+
+typedef struct {
+    long long submitted, completed, failed;
+    long long batches;      /* batches launched */
+    double mean_batch;      /* requests per batch */
+    double p50_us, p99_us, mean_us, max_us;  /* latency, submit to completion */
+    double flops;           /* GEMM FLOPs of completed requests */
+    double span_s;          /* first submit to last completion */
+    long long peak_bytes;   /* most device bytes held by admitted requests at once */
+} fg_server_stats;
+
+int fg_server_create(const fg_server_opts *opts, fg_server *out);
+/* Queues a request; returns its id (>= 0) or a negative fg_status. The request's
+ * buffers must stay valid until fg_server_wait returns for it. Thread-safe. */
+long long fg_server_submit(fg_server s, const fg_request *r);
+/* Blocks until request `id` is done; its latency in microseconds (may be NULL).
+ * Returns the request's status; the id is then forgotten. */
+int fg_server_wait(fg_server s, long long id, double *latency_us);
+/* Blocks until every submitted request is done. */
+int fg_server_drain(fg_server s);
+int fg_server_get_stats(fg_server s, fg_server_stats *out);
+/* Clears the latency record and counters (between the points of a rate sweep). */
+int fg_server_reset_stats(fg_server s);
+/* Drains, stops the loop's threads and frees its device memory. */
+int fg_server_destroy(fg_server s);
+
 /* Wait for all of the library's work on the current device and report any
  * kernel-side error since the last fg_sync (then cleared). */
 int fg_sync(void);
