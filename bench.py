@@ -1,7 +1,7 @@
 """Benchmark of the flashgemm hot path on B200: one JSON line on stdout.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload bf16-chain|int8-chain|f32-gemm|bf16-gemm|int8-gemm|f32-groups]
+                    [--workload bf16-chain|int8-chain|f32-gemm|bf16-gemm|int8-gemm|f32-groups|serve]
 
 A step is one pass of the hot path over one batch: by default the BF16 chain
 of three GEMMs C = A3*(A2*(A1*B)) with B 1024 x 4096 (the activations X
@@ -27,6 +27,12 @@ plus tall-skinny chains of 65536 columns with 64 x 64 weights), N(0,1)/sqrt(K)
 entries, run as one graph-captured grouped 3xTF32 launch; the same group
 through the plain FP32 kernel beside it, and both errors against FP64 on a
 seeded sample of the chains.
+
+--workload serve: the library's serving loop under Poisson arrivals of chain
+requests (length U{2..6}, dimensions and activation columns log-uniform on
+multiples of 16 in [64, 4096], 50/30/20 BF16/INT8/FP32 over 64 resident
+weight sets), replayed from native code at fractions of the capacity measured
+on a burst; p50/p99 latency and throughput per rate.
 """
 import argparse
 import json
@@ -566,6 +572,311 @@ def run_groups(args, world, rank, local_rank):
     return 0
 
 
+# ---------------------------------------------------------------- serving stream
+
+SERVE_SETS = 64
+SERVE_MIX = (("bf16", 0.5), ("int8", 0.3), ("f32", 0.2))
+
+
+def serve_sets(seed):
+    """64 weight sets: dtypes in the 50/30/20 BF16/INT8/FP32 mix, chain length
+    U{2..6}, dimensions log-uniform on multiples of 16 in [64, 4096]."""
+    rng = np.random.default_rng(seed)
+    counts = {"bf16": 32, "int8": 19, "f32": 13}
+    dts = [d for d, c in counts.items() for _ in range(c)]
+    rng.shuffle(dts)
+
+    def dim():
+        v = int(16 * round(float(np.exp(rng.uniform(np.log(64), np.log(4096)))) / 16))
+        return min(max(v, 64), 4096)
+
+    out = []
+    for dt in dts:
+        n = int(rng.integers(2, 7))
+        dims = [dim() for _ in range(n + 1)]
+        out.append((dt, dims[0], dims[1:]))
+    return out
+
+
+def serve_requests(seed, sets, count):
+    """(set index, N) per request: dtype by the mix, a set of that dtype
+    uniformly, N log-uniform on multiples of 16 in [64, 4096]."""
+    rng = np.random.default_rng(seed)
+    by = {d: [i for i, s in enumerate(sets) if s[0] == d] for d, _ in SERVE_MIX}
+    dts = rng.choice([d for d, _ in SERVE_MIX], size=count, p=[p for _, p in SERVE_MIX])
+    out = []
+    for d in dts:
+        i = int(rng.choice(by[str(d)]))
+        N = int(16 * round(float(np.exp(rng.uniform(np.log(64), np.log(4096)))) / 16))
+        out.append((i, min(max(N, 64), 4096)))
+    return out
+
+
+def serve_flops(sets, reqs):
+    return [flops_of(N, sets[i][1], sets[i][2]) for i, N in reqs]
+
+
+def serve_cpu(sets, reqs, host, steps=None, budget_s=12.0):
+    """The reference's chains (or the C port) on sampled requests, all host threads."""
+    oracle, kind, model, amx = reference_runner()
+    threads = os.cpu_count() or 1
+    fl = sum(serve_flops(sets, reqs))
+
+    def one():
+        for i, N in reqs:
+            dt, K1, Ms = sets[i]
+            B, As = host[(i, N)]
+            Ks = [K1] + Ms[:-1]
+            if kind == "reference":
+                oracle.ref_chain(dt, B, As, N, Ms, Ks, threads=threads)
+            else:
+                oracle.chain(dt, B, As, N, Ms, Ks, mode=oracle.REF, threads=threads)
+    one()
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while True:
+        t0 = time.perf_counter()
+        one()
+        times.append(time.perf_counter() - t0)
+        if steps is not None:
+            if len(times) >= steps:
+                break
+        elif len(times) >= 3 and time.perf_counter() > t_end:
+            break
+    med = statistics.median(times)
+    descr = {"kind": kind, "cores": threads, "cpu": model, "amx_available": amx,
+             "amx_used": False,
+             "sample": f"{len(reqs)} requests of the stream run one after another "
+                       f"({fl / 1e9:.1f} GFLOP per step), median of {len(times)} steps"}
+    return fl / med / 1e12, descr, times
+
+
+def serve_cpu_inputs(sets, reqs, seed):
+    rng = np.random.default_rng(seed)
+    host = {}
+    for i, N in reqs:
+        dt, K1, Ms = sets[i]
+        B, As, _ = make_inputs(dt, N, K1, Ms, int(rng.integers(1 << 30)))
+        host[(i, N)] = (B, As)
+    return host
+
+
+def run_serve(args, world, rank, local_rank):
+    seed = 777
+    sets = serve_sets(seed)
+    nreq = args.serve_requests
+    cpu_sample = serve_requests(seed + 5, sets, 24)
+    config = {"workload": "serving stream: Poisson arrivals of chain requests, chain length "
+                          "U{2..6}, dims log-uniform on multiples of 16 in [64, 4096], dtype mix "
+                          "50% BF16 / 30% INT8 / 20% FP32 (3xTF32) over 64 resident weight sets; "
+                          "activations and results resident in HBM",
+              "requests_per_rate": nreq, "weight_sets": len(sets),
+              "server": {"max_batch": 64, "slots": 2, "max_wait_us": 200},
+              "l2": "inputs of the stream far exceed L2; no flush between requests",
+              "parallelism": f"dp{world} (each rank serves its own stream)"}
+    metric = "served chain requests TFLOP/s (p50/p99 latency beside)"
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        host = serve_cpu_inputs(sets, cpu_sample, seed + 6)
+        tf, descr, times = serve_cpu(sets, cpu_sample, host, steps=args.steps)
+        line = {"impl": "reference", "metric": metric, "value": tf, "unit": "TFLOP/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * statistics.median(times), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "bf16/int8/f32 mix",
+                "data": "synthetic (seeded)", "config": config,
+                "cpu_baseline": dict(descr, value=tf, unit="TFLOP/s"),
+                "e2e": {"value": tf, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    import flashgemm_b200 as fg
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    fg.lib()
+    fg.set_semantics("ref")
+    fg.set_f32_algo("3xtf32")
+    tdt = {"bf16": torch.bfloat16, "int8": torch.int8, "f32": torch.float32}
+    W, Bs, Cs = [], [], []
+    t_gen = time.perf_counter()
+    for j, (dt, K1, Ms) in enumerate(sets):
+        g = torch.Generator(device=dev).manual_seed(seed + j + 1000 * rank)
+        Ks = [K1] + Ms[:-1]
+        ws = []
+        for m, k in zip(Ms, Ks):
+            if dt == "int8":
+                a = torch.randint(-127, 128, (m, k), generator=g, device=dev, dtype=torch.int8)
+            else:
+                a = (torch.randn(m, k, generator=g, device=dev) / float(np.sqrt(k))).to(tdt[dt])
+                if dt == "bf16":
+                    a = a.view(torch.int16)
+            ws.append(fg.Weights(dt, a))
+            del a
+        W.append(ws)
+        if dt == "int8":
+            b = torch.randint(-127, 128, (K1 * 4096,), generator=g, device=dev, dtype=torch.int8)
+        else:
+            b = torch.randn(K1 * 4096, generator=g, device=dev).to(tdt[dt])
+            if dt == "bf16":
+                b = b.view(torch.int16)
+        Bs.append(b)
+        Cs.append([torch.empty(Ms[-1] * 4096, dtype=torch.int32 if dt == "int8" else torch.float32,
+                               device=dev) for _ in range(4)])
+    torch.cuda.synchronize(dev)
+    t_gen = time.perf_counter() - t_gen
+    weight_bytes = sum(w.nbytes for ws in W for w in ws)
+    ring = [0] * len(sets)
+
+    def materialise(reqs):
+        out = []
+        for i, N in reqs:
+            dt, K1, Ms = sets[i]
+            c = Cs[i][ring[i] % 4]
+            ring[i] += 1
+            out.append((dt, W[i], Bs[i][:K1 * N].view(K1, N), c[:Ms[-1] * N].view(Ms[-1], N)))
+        return out
+
+    srv = fg.Server(max_batch=64, slots=2, max_wait_us=200)
+
+    def run_point(reqs, at_us, prof=False):
+        if dist:
+            dist.barrier()
+        fl = serve_flops(sets, reqs)
+        mats = materialise(reqs)
+        srv.reset_stats()
+        l0 = fg.kernel_launches()
+        if prof:
+            fg.profile_begin()
+        ids = srv.replay(mats, at_us)
+        srv.drain()
+        st = srv.stats()
+        kernels = None
+        if prof:
+            torch.cuda.synchronize(dev)
+            kernels = {name: fg.profile_query(k) for name, k in
+                       (("bf16", fg.FG_PK_TC_BF16), ("int8", fg.FG_PK_TC_I8),
+                        ("tf32x3", fg.FG_PK_TC_TF32X3))}
+            fg.profile_end()
+        launches = fg.kernel_launches() - l0
+        for rid in ids:
+            srv.wait(rid)
+        return st, launches, kernels, sum(fl)
+
+    # warm-up (pool, tensor-map encoder, code paths), then capacity from a burst
+    warm = serve_requests(seed + 1, sets, 400)
+    run_point(warm, [0.0] * len(warm))
+    burst = serve_requests(seed + 2, sets, min(4000, nreq))
+    st, _, _, fl = run_point(burst, [0.0] * len(burst))
+    capacity = st["completed"] / st["span_s"]
+    points = []
+    sampler = ClockSampler(torch.cuda.current_device())
+    launches_total = 0
+    kernels = None
+    rng = np.random.default_rng(seed + 3)
+    with sampler:
+        for k, frac in enumerate(args.serve_rates):
+            rate = frac * capacity
+            reqs = serve_requests(seed + 10 + k, sets, nreq)
+            at = np.cumsum(rng.exponential(1e6 / rate, size=nreq))
+            prof = k == len(args.serve_rates) - 1
+            st, launches, kern, fl = run_point(reqs, at.tolist(), prof=prof)
+            launches_total += launches
+            if prof:
+                kernels = kern
+            points.append({"offered_req_s": rate, "offered_frac_of_capacity": frac,
+                           "served_req_s": st["completed"] / st["span_s"],
+                           "tflops": st["flops"] / st["span_s"] / 1e12,
+                           "p50_us": st["p50_us"], "p99_us": st["p99_us"],
+                           "mean_us": st["mean_us"], "max_us": st["max_us"],
+                           "batches": st["batches"], "mean_batch": st["mean_batch"],
+                           "failed": st["failed"], "peak_bytes": st["peak_bytes"]})
+
+    # end to end: host (pinned) activations in and results out inside each request
+    e2e_n = min(nreq, 4000)
+    reqs = serve_requests(seed + 50, sets, e2e_n)
+    hB = [torch.empty(b.numel(), dtype=b.dtype, pin_memory=True) for b in Bs]
+    for h, b in zip(hB, Bs):
+        h.copy_(b)
+    hC = [torch.empty(Cs[i][0].numel(), dtype=Cs[i][0].dtype, pin_memory=True)
+          for i in range(len(sets))]
+    mats, h2d, d2h = [], 0, 0
+    for i, N in reqs:
+        dt, K1, Ms = sets[i]
+        b = hB[i][:K1 * N].view(K1, N).numpy()
+        c = hC[i][:Ms[-1] * N].view(Ms[-1], N).numpy()
+        mats.append((dt, W[i], b, c))
+        h2d += b.nbytes
+        d2h += c.nbytes
+    rate = 0.6 * capacity
+    at = np.cumsum(rng.exponential(1e6 / rate, size=e2e_n))
+    srv.reset_stats()
+    ids = srv.replay(mats, at.tolist())
+    srv.drain()
+    st_e2e = srv.stats()
+    for rid in ids:
+        srv.wait(rid)
+    srv.close()
+    for ws in W:
+        for w in ws:
+            w.release()
+    if dist:
+        t = torch.tensor([points[-1]["tflops"]], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    top = points[-1]
+    peaks, peak_src = load_peaks()
+    main = max(kernels.items(), key=lambda kv: kv[1][0]) if kernels else None
+    roofline = None
+    if main and main[1][0] > 0:
+        name, (k_ms, k_n, k_fl) = main
+        peak = {"bf16": peaks["bf16_tflops"], "int8": 2 * peaks["bf16_tflops"],
+                "tf32x3": peaks["bf16_tflops"] / 6.0}[name]
+        ach = k_fl / (k_ms / 1e3) / 1e12
+        roofline = {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                    "frac": ach / peak, "traffic": None,
+                    "kernel": f"grouped {name} kernel (the class with the most device time)",
+                    "launches_timed": k_n, "avg_launch_us": 1e3 * k_ms / k_n,
+                    "peak_source": ("bf16_tflops" if name == "bf16" else
+                                    "2 x bf16_tflops" if name == "int8" else
+                                    "bf16_tflops / 2 / 3") + f"; {peak_src}"}
+    line = {"metric": metric, "value": world * top["tflops"], "unit": "TFLOP/s", "n_gpus": world,
+            "steps": len(points), "warmup": 1, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16/int8/f32(3xTF32) mix",
+            "data": "synthetic (seeded; no dataset involved)", "config": config,
+            "clocks": sampler.summary(), "gpu_launches": launches_total,
+            "latency": {"p50_us": top["p50_us"], "p99_us": top["p99_us"],
+                        "at_offered_frac_of_capacity": top["offered_frac_of_capacity"]},
+            "capacity_req_s": capacity, "points": points,
+            "e2e": {"value": st_e2e["flops"] / st_e2e["span_s"] / 1e12 * world, "unit": "TFLOP/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "step": f"{e2e_n} requests at 0.6 x capacity",
+                    "p50_us": st_e2e["p50_us"], "p99_us": st_e2e["p99_us"],
+                    "api": "fg_server_* with pinned host activations and results"},
+            "roofline": roofline,
+            "kernels": {k: {"ms": v[0], "launches": v[1],
+                            "tflops": v[2] / (v[0] / 1e3) / 1e12 if v[0] else None}
+                        for k, v in (kernels or {}).items()},
+            "resident": {"weight_bytes": weight_bytes, "setup_s": t_gen}}
+    if world == 1:
+        host = serve_cpu_inputs(sets, cpu_sample, seed + 6)
+        tf, descr, _ = serve_cpu(sets, cpu_sample, host, budget_s=args.cpu_budget)
+        line["cpu_baseline"] = dict(descr, value=tf, unit="TFLOP/s")
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -575,7 +886,11 @@ def main():
                     help="untimed steps (default 20; f32-groups 3)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="bf16-chain",
-                    choices=list(WORKLOADS) + ["f32-groups"])
+                    choices=list(WORKLOADS) + ["f32-groups", "serve"])
+    ap.add_argument("--serve-requests", type=int, default=20000,
+                    help="serve: Poisson requests per rate point")
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[0.3, 0.6, 0.9],
+                    help="serve: offered rates as fractions of the measured capacity")
     ap.add_argument("--e2e-steps", type=int, default=None,
                     help="steps of the host-buffer C-ABI measurement (default: min(steps, 200))")
     ap.add_argument("--cpu-budget", type=float, default=12.0,
@@ -592,6 +907,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if grouped:
         return run_groups(args, world, rank, local_rank)
+    if args.workload == "serve":
+        return run_serve(args, world, rank, local_rank)
     dt, N, K1, Ms = WORKLOADS[args.workload]
     metric = {"f32": "FP32 GEMM TFLOP/s"}.get(dt, "fused GEMM-chain TFLOP/s")
     config = {"workload": DESCR[args.workload], "dtype": dt, "N": N, "K1": K1, "M": Ms,

@@ -530,6 +530,34 @@ class Server:
             raise FlashgemmError(st, last_error())
         return lat.value
 
+    def replay(self, requests, at_us):
+        """Submit requests [(dtype, weights, B, C), ...] at the given offsets
+        (microseconds from now, non-decreasing) from native code; returns the ids."""
+        L = lib()
+        n = len(requests)
+        arr = (_Request * n)()
+        keep = []
+        for r, (dtype, weights, B, C) in zip(arr, requests):
+            host = isinstance(B, np.ndarray)
+            hs = (_P * len(weights))(*[w.handle for w in weights])
+            keep.append((hs, B, C, weights))
+            r.dtype, r.num_gemm, r.W = _DT[dtype], len(weights), ctypes.cast(hs, _P)
+            r.N = int(B.shape[1])
+            r.B = B.ctypes.data if host else B.data_ptr()
+            r.C = C.ctypes.data if host else C.data_ptr()
+            r.where = FG_MEM_HOST if host else FG_MEM_DEVICE
+        at = (ctypes.c_double * n)(*[float(x) for x in at_us])
+        ids = (ctypes.c_longlong * n)()
+        L.fg_server_replay.argtypes = [_P, _P, ctypes.c_int, _P, _P]
+        st = L.fg_server_replay(self.handle, arr, n, at, ids)
+        if st != FG_OK:
+            raise FlashgemmError(st, last_error())
+        out = list(ids)
+        for rid, k in zip(out, keep):
+            if rid >= 0:
+                self._keep[rid] = k
+        return out
+
     def drain(self):
         st = lib().fg_server_drain(self.handle)
         if st != FG_OK:

@@ -1398,24 +1398,19 @@ size_t group_buf_bytes(int dtype, int algo, int nchains, const fg_chain_desc *ch
     return need;
 }
 
-// Cost model of a grouped launch (microseconds): per tile, k-blocks times the
-// MMA time of one k-block on the tile's SMs (at the measured dense BF16 rate
-// per SM; INT8 k-blocks hold twice the K at twice the rate, TF32 runs at half
-// the rate, 3xTF32 issues three MMAs) plus the part of the epilogue that does
-// not overlap; a dependent tile starts 2 us after its column block is done,
-// and every extra launch costs 3 us.
-double model_tile_us(int kernel, int op, long K)
-{
-    const double kb_elems = op == OP_I8 ? 128.0 : op == OP_BF16 ? 64.0 : 32.0;
-    const double kb = std::ceil((double)K / kb_elems);
-    const double per_sm_tflops = 1600.0 / 148.0;
-    double m = 128.0, n = group_tile_n(kernel, op), sms = 1.0;
-    if (op != OP_TF32X3 && kernel == GK_PAIR) m = 256.0, n = 256.0, sms = 2.0;
-    double rate = per_sm_tflops * sms * (op == OP_I8 ? 2.0 : op == OP_TF32X3 ? 0.5 / 3.0 : 1.0);
-    const double t_kb = 2.0 * m * n * kb_elems / (rate * 1e6);
-    return kb * t_kb + 0.5;
-}
-
+// Cost model of a grouped launch (microseconds), closed form so that it costs
+// far less than the launch it chooses for. A tile takes the longer of its MMA
+// time (k-blocks x one k-block on the tile's SMs at the measured dense BF16
+// rate per SM; INT8 k-blocks hold twice the K at twice the rate, TF32 runs at
+// half the rate and 3xTF32 issues three MMAs) and its epilogue (output bytes
+// per SM at about 16 GB/s per SM, the staged drain's measured rate), plus
+// 0.3 us. Levels: each level takes max(its work / workers, its longest tile)
+// plus 3 us of launch; fused: max(all work / workers, the longest chain's
+// tiles back to back with 2 us hand-offs). The result is divided by the
+// kernel's efficiency measured on the 512-chain grouped workload relative to
+// the best kernel for that operand type (B200: BF16 pair 1.0, 128x256 0.90,
+// 128x128 0.74; INT8 pair 0.90, 128x256 1.0, 128x128 0.82), and fused runs pay
+// the 8% their dependency waits cost there.
 struct ModelStage {
     long M, N, K;
     int prev, depth;
@@ -1423,34 +1418,46 @@ struct ModelStage {
 
 double model_makespan(int kernel, int order, int op, int sms, const std::vector<ModelStage> &st)
 {
-    const int units = (op != OP_TF32X3 && kernel == GK_PAIR) ? sms / 2 : sms;
-    const int tm = (op != OP_TF32X3 && kernel == GK_PAIR) ? 256 : 128;
-    const int tn = (op != OP_TF32X3 && kernel == GK_PAIR) ? 256 : group_tile_n(kernel, op);
+    const bool pair = op != OP_TF32X3 && kernel == GK_PAIR;
+    const double units = pair ? sms / 2 : sms;
+    const double tm = pair ? 256 : 128, tn = pair ? 256 : group_tile_n(kernel, op);
+    const double sm_per_tile = pair ? 2.0 : 1.0;
+    const double kb_elems = op == OP_I8 ? 128.0 : op == OP_BF16 ? 64.0 : 32.0;
+    const double rate = 1600.0 / 148.0 * sm_per_tile *
+                        (op == OP_I8 ? 2.0 : op == OP_TF32X3 ? 0.5 / 3.0 : 1.0);  // TFLOP/s
+    const double t_kb = 2.0 * tm * tn * kb_elems / (rate * 1e6);
+    const double out_elt = op == OP_I8 ? 1.0 : op == OP_BF16 ? 2.0 : 8.0;
+    const double t_epi = tm * tn * out_elt / sm_per_tile / 16e3;
+    std::vector<double> tile(st.size()), work(st.size());
     int maxd = 0;
-    for (auto &x : st) maxd = std::max(maxd, x.depth);
-    double total = 0.0;
-    for (int lv = 0; lv <= (order == FG_ORDER_LEVELS ? maxd : 0); ++lv) {
-        std::vector<SchedStage> ss;
-        std::vector<int> remap(st.size(), -1);
-        int off = 0;
-        for (size_t i = 0; i < st.size(); ++i) {
-            if (order == FG_ORDER_LEVELS && st[i].depth != lv) continue;
-            const int tiles_m = (int)((st[i].M + tm - 1) / tm), tiles_n = (int)((st[i].N + tn - 1) / tn);
-            const int prev = order == FG_ORDER_LEVELS ? -1 : (st[i].prev >= 0 ? remap[st[i].prev] : -1);
-            remap[i] = (int)ss.size();
-            ss.push_back(SchedStage{tiles_m, tiles_n, prev, off, model_tile_us(kernel, op, st[i].K)});
-            off += tiles_n;
-        }
-        long tiles = 0;
-        for (auto &x : ss) tiles += (long)x.tiles_m * x.tiles_n;
-        const int u = (int)std::min<long>(units, std::max<long>(tiles, 1));
-        std::vector<int> o;
-        std::vector<WorkEntry> e;
-        double span = 0.0;
-        list_schedule(ss.data(), (int)ss.size(), u, 2.0, o, e, &span);
-        total += span + 3.0;
+    for (size_t i = 0; i < st.size(); ++i) {
+        const double kb = std::ceil((double)st[i].K / kb_elems);
+        tile[i] = std::max(kb * t_kb, t_epi) + 0.3;
+        work[i] = tile[i] * std::ceil(st[i].M / tm) * std::ceil(st[i].N / tn);
+        maxd = std::max(maxd, st[i].depth);
     }
-    return total;
+    double eff = 1.0;
+    if (op == OP_BF16) eff = kernel == GK_PAIR ? 1.0 : kernel == GK_SINGLE_256 ? 0.90 : 0.74;
+    if (op == OP_I8) eff = kernel == GK_PAIR ? 0.90 : kernel == GK_SINGLE_256 ? 1.0 : 0.82;
+    double t = 0.0;
+    if (order == FG_ORDER_LEVELS) {
+        std::vector<double> lw(maxd + 1, 0.0), lt(maxd + 1, 0.0);
+        for (size_t i = 0; i < st.size(); ++i) {
+            lw[st[i].depth] += work[i];
+            lt[st[i].depth] = std::max(lt[st[i].depth], tile[i]);
+        }
+        for (int l = 0; l <= maxd; ++l) t += std::max(lw[l] / units, lt[l]) + 3.0;
+    } else {
+        double total = 0.0, crit = 0.0;
+        std::vector<double> path(st.size(), 0.0);
+        for (size_t i = 0; i < st.size(); ++i) {
+            total += work[i];
+            path[i] = (st[i].prev >= 0 ? path[st[i].prev] + 2.0 : 0.0) + tile[i];
+            crit = std::max(crit, path[i]);
+        }
+        t = std::max(1.08 * total / units, crit) + 3.0;
+    }
+    return t / eff;
 }
 
 // ---------------------------------------------------------------- autotuner memory
@@ -2428,6 +2435,23 @@ FG_EXPORT int fg_server_wait(fg_server s, long long id, double *latency_us)
     s->reqs.erase(it);
     delete q;
     if (st) return fail(st, "request %lld failed (status %d)", id, st);
+    return ok();
+}
+
+FG_EXPORT int fg_server_replay(fg_server s, const fg_request *reqs, int n, const double *at_us,
+                               long long *ids)
+{
+    if (!s || (n > 0 && (!reqs || !at_us || !ids))) return fail(FG_ERR_INVALID, "null pointer");
+    const double t0 = now_us();
+    for (int i = 0; i < n; ++i) {
+        const double due = t0 + at_us[i];
+        double t = now_us();
+        if (due - t > 300.0)
+            std::this_thread::sleep_for(std::chrono::microseconds((long)(due - t - 200.0)));
+        while (now_us() < due) {
+        }
+        ids[i] = fg_server_submit(s, reqs + i);
+    }
     return ok();
 }
 

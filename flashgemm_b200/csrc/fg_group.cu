@@ -403,10 +403,11 @@ void list_schedule(const SchedStage *st, int n, int units, double handoff, std::
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return depth[x] < depth[y]; });
     std::vector<double> block_done(nblocks, 0.0);
     std::vector<std::vector<WorkEntry>> per(units);
-    // Small problems: scan every worker, ties to the lowest index. Large ones:
-    // a heap of (free time, worker); a tile whose input is not ready before the
-    // earliest free worker takes that worker.
-    const bool scan = (double)units * (double)total <= 4e6;
+    // Small problems (one chain's few hundred tiles): scan every worker, ties to
+    // the lowest index. Larger ones: a heap of (free time, worker), O(log workers)
+    // per tile; a tile whose input is not ready before the earliest free worker
+    // takes that worker.
+    const bool scan = (double)units * (double)total <= 2e5;
     std::vector<double> free_at(units, 0.0);
     using Slot = std::pair<double, int>;
     std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;

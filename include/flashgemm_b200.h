@@ -233,6 +233,13 @@ long long fg_server_submit(fg_server s, const fg_request *r);
 /* Blocks until request `id` is done; its latency in microseconds (may be NULL).
  * Returns the request's status; the id is then forgotten. */
 int fg_server_wait(fg_server s, long long id, double *latency_us);
+/* Trace replay: submits reqs[i] at at_us[i] microseconds after the call (offsets
+ * non-decreasing), from the calling thread, and stores the ids in ids[i] (a
+ * negative fg_status where a submit was refused). Returns once all are
+ * submitted, not done: a load generator for measuring the loop under a given
+ * arrival process. */
+int fg_server_replay(fg_server s, const fg_request *reqs, int n, const double *at_us,
+                     long long *ids);
 /* Blocks until every submitted request is done. */
 int fg_server_drain(fg_server s);
 int fg_server_get_stats(fg_server s, fg_server_stats *out);
