@@ -67,6 +67,11 @@ __global__ void __launch_bounds__(kThreads, 1)
             mbar_init(&bars->acc_full[a], 1);
             mbar_init(&bars->acc_empty[a], 4 * 32);
         }
+        if constexpr (T::split)
+            for (int a = 0; a < 2; ++a) {
+                mbar_init(&bars->full[6 + a], 1);        // correction ready
+                mbar_init(&bars->empty[6 + a], 4 * 32);  // correction drained
+            }
         mbar_init(&bars->mma_done, 1);
         bars->abort = 0;
         fence_mbar_init();
@@ -144,7 +149,18 @@ __global__ void __launch_bounds__(kThreads, 1)
             uint32_t ph = 0;
             int acc = 0;
             uint32_t acc_ph = 0;
+            int cb = 0;  // 3xTF32: correction accumulator of this tile
+            uint32_t cb_ph = 0;
             for (int t = blockIdx.x; t < num_tiles; t += gridDim.x) {
+                uint32_t c_tmem = 0;
+                if constexpr (T::split) {
+                    if (!mbar_wait(&bars->empty[6 + cb], cb_ph ^ 1, p.status, KERR_WAIT_ACC_EMPTY)) {
+                        set_abort(bars);
+                        goto mma_done;
+                    }
+                    tc_fence_after();
+                    c_tmem = tmem_base + G::CORR_COLS + cb * T::BN;
+                }
                 // one accumulator hand-off per chunk of k-blocks (the whole K unless
                 // the epilogue promotes partial sums, see kchunk)
                 for (int kc = 0; kc < num_kb; kc += kchunk) {
@@ -178,10 +194,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                                 const uint64_t bd_lo =
                                     smem_desc(b_addr + lo_off + k * G::B_KSTEP_BYTES,
                                               G::BOX_BYTES, G::B_SBO, T::b_layout);
-                                // hi*lo + lo*hi into the correction accumulator, whose
-                                // rounding is 2^-11 smaller; hi*hi alone into the main one
-                                tc_mma<T::kind>(d_tmem + BN, ad, bd_lo, T::idesc, accumulate);
-                                tc_mma<T::kind>(d_tmem + BN, ad_lo, bd, T::idesc, 1);
+                                // hi*lo + lo*hi into the tile's correction accumulator,
+                                // whose rounding is 2^-11 smaller; hi*hi alone into the
+                                // chunk's main one
+                                tc_mma<T::kind>(c_tmem, ad, bd_lo, T::idesc, (kb | k) != 0);
+                                tc_mma<T::kind>(c_tmem, ad_lo, bd, T::idesc, 1);
                                 tc_mma<T::kind>(d_tmem, ad, bd, T::idesc, accumulate);
                             } else {
                                 tc_mma<T::kind>(d_tmem, ad, bd, T::idesc, accumulate);
@@ -199,6 +216,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                         acc_ph ^= 1;
                     }
                 }
+                if constexpr (T::split) {
+                    tc_commit(&bars->full[6 + cb]);
+                    if (++cb == 2) {
+                        cb = 0;
+                        cb_ph ^= 1;
+                    }
+                }
                 if (aborted(bars)) break;
             }
         mma_done:
@@ -212,6 +236,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         int acc = 0;
         uint32_t acc_ph = 0;
         if constexpr (T::split) {
+            int cb = 0;
+            uint32_t cb_ph = 0;
             for (int t = blockIdx.x; t < num_tiles; t += gridDim.x) {
                 const int m0 = (t / tiles_n) * kBM;
                 const int n0 = (t % tiles_n) * BN;
@@ -232,23 +258,39 @@ __global__ void __launch_bounds__(kThreads, 1)
                         tmem_base + acc * G::ACC_COLS + ((uint32_t)(quarter * 32) << 16);
 #pragma unroll
                     for (int c = 0; c < BN / 32; ++c) {
+                        uint32_t v[32];
+                        tmem_ld_32x32b_x32(t_row + c * 32, v);
+                        tmem_ld_wait();
 #pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            uint32_t v[16], w[16];
-                            tmem_ld_32x32b_x16(t_row + c * 32 + 16 * h, v);
-                            tmem_ld_32x32b_x16(t_row + BN + c * 32 + 16 * h, w);
-                            tmem_ld_wait();
-#pragma unroll
-                            for (int j = 0; j < 16; ++j)
-                                sum[c][16 * h + j] = sum[c][16 * h + j] +
-                                                     (__uint_as_float(v[j]) + __uint_as_float(w[j]));
-                        }
+                        for (int j = 0; j < 32; ++j) sum[c][j] = sum[c][j] + __uint_as_float(v[j]);
                     }
                     tc_fence_before();
                     mbar_arrive(&bars->acc_empty[acc]);
                     if (++acc == 2) {
                         acc = 0;
                         acc_ph ^= 1;
+                    }
+                }
+                // the tile's correction terms, added once
+                if (ok && !mbar_wait(&bars->full[6 + cb], cb_ph, p.status, KERR_WAIT_ACC_FULL))
+                    ok = false;
+                if (ok) {
+                    tc_fence_after();
+                    const uint32_t t_row = tmem_base + G::CORR_COLS + cb * BN +
+                                           ((uint32_t)(quarter * 32) << 16);
+#pragma unroll
+                    for (int c = 0; c < BN / 32; ++c) {
+                        uint32_t w[32];
+                        tmem_ld_32x32b_x32(t_row + c * 32, w);
+                        tmem_ld_wait();
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) sum[c][j] = sum[c][j] + __uint_as_float(w[j]);
+                    }
+                    tc_fence_before();
+                    mbar_arrive(&bars->empty[6 + cb]);
+                    if (++cb == 2) {
+                        cb = 0;
+                        cb_ph ^= 1;
                     }
                 }
                 if (!ok) {

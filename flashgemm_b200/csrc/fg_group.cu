@@ -47,8 +47,11 @@ struct GroupGeo {
     static constexpr int MMAS_PER_STAGE = kRowBytes / MMA_K_BYTES;
     static constexpr int B_KSTEP_BYTES = (MMA_K_BYTES / T::elt) * kRowBytes;
     static constexpr int B_SBO = T::b_layout == SMEM_SW128_32B ? 512 : 1024;
-    static constexpr int ACC_COLS = (T::split ? 2 : 1) * BN;
-    static constexpr int TMEM_COLS = 2 * ACC_COLS;
+    // TMEM: two accumulators of BN columns; 3xTF32 adds two correction
+    // accumulators (hi*lo + lo*hi, one per tile in flight) at CORR_COLS
+    static constexpr int ACC_COLS = BN;
+    static constexpr int CORR_COLS = 2 * BN;
+    static constexpr int TMEM_COLS = (T::split ? 4 : 2) * BN;
     static constexpr int STAGING_BYTES = T::split ? 0 : kEpiStagingBytes;
     static constexpr int SMEM_BYTES = S * STAGE_BYTES + STAGING_BYTES + 1024 + 256;
     static constexpr uint32_t idesc = OP == OP_BF16 ? make_idesc(1, 1, 1, 0, 1, kBM, BN)
@@ -56,7 +59,7 @@ struct GroupGeo {
                                                     : make_idesc(1, 2, 2, 0, 1, kBM, BN);
     static_assert(SMEM_BYTES <= 232448, "shared memory per CTA");
     static_assert(TMEM_COLS <= 512, "TMEM columns");
-    static_assert(S <= 8, "barrier slots");
+    static_assert(S <= (T::split ? 6 : 8), "barrier slots (3xTF32 uses the last two pairs)");
 };
 
 struct alignas(64) GroupStage {
@@ -108,6 +111,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
             mbar_init(&bars->acc_full[a], 1);
             mbar_init(&bars->acc_empty[a], kGroupDonePerTile);  // one arrival per epilogue warp
         }
+        if constexpr (T::split)
+            for (int a = 0; a < 2; ++a) {
+                mbar_init(&bars->full[6 + a], 1);                    // correction ready
+                mbar_init(&bars->empty[6 + a], kGroupDonePerTile);   // correction drained
+            }
         mbar_init(&bars->mma_done, 1);
         bars->abort = 0;
         fence_mbar_init();
@@ -214,12 +222,24 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
             uint32_t ph = 0;
             int acc = 0;
             uint32_t acc_ph = 0;
+            int cb = 0;          // 3xTF32: correction accumulator of this tile
+            uint32_t cb_ph = 0;
             for (int q = q_begin; q < q_end; ++q) {
                 const GroupStage &cs = g.st[g.sched[q].stage];
                 const int num_kb = (cs.a.K + G::BK - 1) / G::BK;
-                // 3xTF32 hands partial sums to the epilogue every kchunk k-blocks (FP32
-                // promotion in registers, as in the one-stage kernel)
+                // 3xTF32 hands the hi*hi partial sum to the epilogue every kchunk
+                // k-blocks (FP32 promotion in registers, as in the one-stage kernel);
+                // the small hi*lo + lo*hi terms accumulate over the whole tile
                 const int kchunk = (T::split && cs.a.kchunk > 0) ? cs.a.kchunk : num_kb;
+                uint32_t c_tmem = 0;
+                if constexpr (T::split) {
+                    if (!mbar_wait(&bars->empty[6 + cb], cb_ph ^ 1, status, KERR_WAIT_ACC_EMPTY)) {
+                        set_abort(bars);
+                        goto mma_done;
+                    }
+                    tc_fence_after();
+                    c_tmem = tmem_base + G::CORR_COLS + cb * BN;
+                }
                 for (int kc = 0; kc < num_kb; kc += kchunk) {
                     if (!mbar_wait(&bars->acc_empty[acc], acc_ph ^ 1, status,
                                    KERR_WAIT_ACC_EMPTY)) {
@@ -251,8 +271,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
                                 const uint64_t bd_lo =
                                     smem_desc(b_addr + lo_off + k * G::B_KSTEP_BYTES,
                                               G::BOX_BYTES, G::B_SBO, T::b_layout);
-                                tc_mma<T::kind>(d_tmem + BN, ad, bd_lo, G::idesc, accumulate);
-                                tc_mma<T::kind>(d_tmem + BN, ad_lo, bd, G::idesc, 1);
+                                tc_mma<T::kind>(c_tmem, ad, bd_lo, G::idesc, (kb | k) != 0);
+                                tc_mma<T::kind>(c_tmem, ad_lo, bd, G::idesc, 1);
                                 tc_mma<T::kind>(d_tmem, ad, bd, G::idesc, accumulate);
                             } else {
                                 tc_mma<T::kind>(d_tmem, ad, bd, G::idesc, accumulate);
@@ -270,6 +290,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
                         acc_ph ^= 1;
                     }
                 }
+                if constexpr (T::split) {
+                    tc_commit(&bars->full[6 + cb]);
+                    if (++cb == 2) {
+                        cb = 0;
+                        cb_ph ^= 1;
+                    }
+                }
                 if (aborted(bars)) break;
             }
         mma_done:
@@ -281,6 +308,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
         const int quarter = warp & 3;
         int acc = 0;
         uint32_t acc_ph = 0;
+        int cb = 0;
+        uint32_t cb_ph = 0;
         uint8_t *staging = smem + S * G::STAGE_BYTES + (warp - 2) * 2 * kStageBufBytes;
         int sbuf = 0;
         for (int q = q_begin; q < q_end; ++q) {
@@ -309,17 +338,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
                         tmem_base + acc * G::ACC_COLS + ((uint32_t)(quarter * 32) << 16);
 #pragma unroll
                     for (int c = 0; c < BN / 32; ++c) {
+                        uint32_t v[32];
+                        tmem_ld_32x32b_x32(t_row + c * 32, v);
+                        tmem_ld_wait();
 #pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            uint32_t v[16], w[16];
-                            tmem_ld_32x32b_x16(t_row + c * 32 + 16 * h, v);
-                            tmem_ld_32x32b_x16(t_row + BN + c * 32 + 16 * h, w);
-                            tmem_ld_wait();
-#pragma unroll
-                            for (int j = 0; j < 16; ++j)
-                                sum[c][16 * h + j] =
-                                    sum[c][16 * h + j] + (__uint_as_float(v[j]) + __uint_as_float(w[j]));
-                        }
+                        for (int j = 0; j < 32; ++j) sum[c][j] = sum[c][j] + __uint_as_float(v[j]);
                     }
                     tc_fence_before();
                     __syncwarp();
@@ -327,6 +350,29 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
                     if (++acc == 2) {
                         acc = 0;
                         acc_ph ^= 1;
+                    }
+                }
+                // the tile's correction terms, added once
+                if (ok && !mbar_wait(&bars->full[6 + cb], cb_ph, status, KERR_WAIT_ACC_FULL))
+                    ok = false;
+                if (ok) {
+                    tc_fence_after();
+                    const uint32_t t_row = tmem_base + G::CORR_COLS + cb * BN +
+                                           ((uint32_t)(quarter * 32) << 16);
+#pragma unroll
+                    for (int c = 0; c < BN / 32; ++c) {
+                        uint32_t w[32];
+                        tmem_ld_32x32b_x32(t_row + c * 32, w);
+                        tmem_ld_wait();
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) sum[c][j] = sum[c][j] + __uint_as_float(w[j]);
+                    }
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&bars->empty[6 + cb]);
+                    if (++cb == 2) {
+                        cb = 0;
+                        cb_ph ^= 1;
                     }
                 }
                 if (ok) {

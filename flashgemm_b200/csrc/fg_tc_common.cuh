@@ -72,10 +72,12 @@ struct Geometry {
     static constexpr int B_KSTEP_BYTES = (MMA_K_BYTES / T::elt) * kRowBytes;
     // stride between k-row groups of the B swizzle atom: 8 rows (16B chunks) or 4 rows (32B)
     static constexpr int B_SBO = T::b_layout == SMEM_SW128_32B ? 512 : 1024;
-    // 3xTF32 keeps the small hi*lo + lo*hi terms in their own accumulator next to
-    // hi*hi: each of the two TMEM buffers is then [hi*hi | corrections].
-    static constexpr int ACC_COLS = (T::split ? 2 : 1) * T::BN;
-    static constexpr int TMEM_COLS = 2 * ACC_COLS;
+    // Two accumulators of BN columns. 3xTF32 keeps the small hi*lo + lo*hi terms
+    // in their own accumulators at CORR_COLS (one per tile in flight), summed over
+    // the whole tile, while hi*hi is handed to the epilogue chunk by chunk.
+    static constexpr int ACC_COLS = T::BN;
+    static constexpr int CORR_COLS = 2 * T::BN;
+    static constexpr int TMEM_COLS = (T::split ? 4 : 2) * T::BN;
     static constexpr int STAGING_BYTES = T::split ? 0 : 4 * 2 * 4096;  // TMA-store epilogue
     static constexpr int SMEM_BYTES =
         T::STAGES * STAGE_BYTES + STAGING_BYTES + 1024 /*align*/ + 256 /*bars*/;
