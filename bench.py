@@ -356,12 +356,14 @@ def group_host_inputs(specs, indices, seed):
 
 def run_groups(args, world, rank, local_rank):
     seed = 4321
-    specs = group_specs(seed)
+    n = max(8, args.group_chains)
+    nsk = max(1, GROUP_SKINNY * n // GROUP_CHAINS)
+    specs = group_specs(seed, count=n, skinny=nsk)
     sample = group_sample(specs, seed + 1)
     total_flops = sum(flops_of(*s) for s in specs)
-    config = {"workload": "512 independent FP32 chains in one graph-captured grouped launch: "
+    config = {"workload": f"{n} independent FP32 chains in one graph-captured grouped launch: "
                           "length U{2..5}, dims log-uniform on multiples of 16 in [64, 4096], "
-                          "activation columns log-uniform in [64, 8192], 8 tall-skinny chains "
+                          f"activation columns log-uniform in [64, 8192], {nsk} tall-skinny chains "
                           "(65536 columns, 64 x 64 weights); N(0,1)/sqrt(K) entries",
               "chains": len(specs), "stages": sum(len(s[2]) for s in specs),
               "gflop_per_step_per_gpu": total_flops / 1e9,
@@ -887,6 +889,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="bf16-chain",
                     choices=list(WORKLOADS) + ["f32-groups", "serve"])
+    ap.add_argument("--group-chains", type=int, default=512,
+                    help="f32-groups: chains in the group (fewer: a small case for profiling)")
     ap.add_argument("--serve-requests", type=int, default=20000,
                     help="serve: Poisson requests per rate point")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[0.3, 0.6, 0.9],

@@ -15,9 +15,9 @@
 // (M_i x 256 per block, too wide for shared memory at these widths) stay in
 // L2 between the two stages that touch them.
 //
-// Every CTA of the grid may wait on another's counters, so the kernel is
-// launched cooperatively (all CTAs co-resident, or the launch fails and the
-// caller falls back to one launch per stage). Every wait is bounded.
+// Every CTA of the grid may wait on another's counters, so the grid never
+// holds more pairs than the device keeps active at once (occupancy API); see
+// launch_pairs for why that suffices. Every wait is bounded.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -340,7 +340,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
             drain_warp<OP, BN>(cs.a, &cs.tm_out, t_row, lane, m0 + quarter * 32, n0, staging,
                                sbuf);
             tc_fence_before();
-            __threadfence();  // direct-store path: this lane's stores before the release
+            // direct-store path: this lane's stores before the release (TMA stores
+            // are ordered by lane 0's bulk wait and fences below)
+            if (!cs.a.tma_store) __threadfence();
             __syncwarp();
             if (lane == 0) {
                 mbar_arrive_cluster(mapa_shared(smem_u32(&bars->acc_empty[acc]), 0));
@@ -455,19 +457,23 @@ template <int OP, bool EXT>
 cudaError_t launch_pairs(const ChainParams &P, int pairs, cudaStream_t s)
 {
     using G = PairGeo<OP>;
+    // Pairs wait on one another, so all must become resident: `pairs` never
+    // exceeds the device's maximum of active clusters for this kernel (occupancy
+    // API), and a pair only ever waits on pairs of its own grid, which run to
+    // completion once resident; pairs held back behind another kernel's CTAs
+    // start when that kernel ends. Every wait is bounded in any case. (No
+    // cooperative flag: cluster launches with it cannot be profiled.)
     cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute attr[2];
+    cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = 2;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    attr[1].id = cudaLaunchAttributeCooperative;  // all pairs resident: they wait on one another
-    attr[1].val.cooperative = 1;
     cfg.blockDim = dim3(kThreads);
     cfg.dynamicSmemBytes = G::SMEM_BYTES;
     cfg.stream = s;
     cfg.attrs = attr;
-    cfg.numAttrs = 2;
+    cfg.numAttrs = 1;
     cfg.gridDim = dim3(2 * pairs);
     return cudaLaunchKernelEx(&cfg, tc_chain_kernel<OP, EXT>, P);
 }

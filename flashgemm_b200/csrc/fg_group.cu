@@ -409,7 +409,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
                 set_abort(bars);
                 break;
             }
-            __threadfence();  // direct stores of this lane before the release
+            // direct stores of this lane before the release (TMA stores are ordered
+            // by lane 0's bulk wait and fences below)
+            if (!cs.a.tma_store) __threadfence();
             __syncwarp();
             if (lane == 0) {
                 // this warp's rows of the tile are in memory: release them
