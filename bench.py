@@ -297,7 +297,7 @@ def group_sample(specs, seed, count=16, skinny=2, max_gflop=20.0):
     small = [i for i, (N, K1, Ms) in enumerate(specs)
              if N != 65536 and flops_of(N, K1, Ms) <= max_gflop * 1e9]
     thin = [i for i, (N, _, _) in enumerate(specs) if N == 65536]
-    pick = list(rng.choice(small, size=min(count, len(small)), replace=False))
+    pick = list(rng.choice(small, size=min(count, len(small)), replace=False)) if small else []
     return sorted(int(i) for i in pick + thin[:skinny])
 
 
@@ -357,7 +357,7 @@ def group_host_inputs(specs, indices, seed):
 def run_groups(args, world, rank, local_rank):
     seed = 4321
     n = max(8, args.group_chains)
-    nsk = max(1, GROUP_SKINNY * n // GROUP_CHAINS)
+    nsk = n if args.skinny_only else max(1, GROUP_SKINNY * n // GROUP_CHAINS)
     specs = group_specs(seed, count=n, skinny=nsk)
     sample = group_sample(specs, seed + 1)
     total_flops = sum(flops_of(*s) for s in specs)
@@ -511,6 +511,38 @@ def run_groups(args, world, rank, local_rank):
     ff_ms, _ = timed(plan2)
     out_ff = sample_out()
     plan2.release()
+
+    # ---- the tall-skinny chains alone: HBM-bound, so GB/s of their fused ideal
+    # (B read once, C written once) against the measured HBM bandwidth
+    thin = [j for j, sp in enumerate(specs) if sp[0] == 65536]
+    skinny = None
+    if thin:
+        sub = [chains[j] for j in thin]
+        sk_bytes = sum(4 * (specs[j][1] + specs[j][2][-1]) * specs[j][0] for j in thin)
+        sk_fl = sum(flops_of(*specs[j]) for j in thin)
+        skinny = {"chains": len(thin), "algorithmic_bytes_per_step": sk_bytes,
+                  "gflop_per_step": sk_fl / 1e9}
+        for algo in ("3xtf32", "ffma"):
+            fg.set_f32_algo(algo)
+            p = fg.Plan("f32", sub)
+            for _ in range(3):
+                p.launch(graph=True)
+            torch.cuda.synchronize(dev)
+            reps, tot = 10, 0.0
+            for i in range(reps):
+                flush.fill_(i & 0xFF)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                p.launch(graph=True)
+                b.record()
+                torch.cuda.synchronize(dev)
+                tot += a.elapsed_time(b)
+            fg.sync()
+            p.release()
+            ms = tot / reps
+            key = "3xtf32" if algo == "3xtf32" else "plain"
+            skinny[f"ms_{key}"] = ms
+            skinny[f"gbs_{key}"] = sk_bytes / (ms / 1e3) / 1e9
     fg.set_f32_algo("3xtf32")
     for c in chains:
         for w in c[3]:
@@ -536,6 +568,11 @@ def run_groups(args, world, rank, local_rank):
     value = world * total_flops * args.steps / (x3_ms / 1e3) / 1e12
     plain = world * total_flops * args.steps / (ff_ms / 1e3) / 1e12
     peaks, peak_src = load_peaks()
+    if skinny:
+        for key in ("3xtf32", "plain"):
+            skinny[f"frac_hbm_{key}"] = skinny[f"gbs_{key}"] / peaks["hbm_gbs"]
+        skinny["hbm_peak_gbs"] = peaks["hbm_gbs"]
+        skinny["peak_source"] = f"hbm_gbs (STREAM-style copy); {peak_src}"
     peak = peaks.get("bf16_tflops") / 2.0 / 3.0
     achieved = k_fl / (k_ms / 1e3) / 1e12 if k_ms > 0 else None
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -559,6 +596,7 @@ def run_groups(args, world, rank, local_rank):
             "plain_fp32": {"value": plain, "unit": "TFLOP/s", "ms_per_step": ff_ms / args.steps,
                            "path": "grouped FFMA kernel, one launch per chain depth"},
             "x3_vs_plain": value / plain,
+            "skinny": skinny,
             "accuracy": {"sample_chains": len(sample),
                          "rel_frob_vs_fp64_3xtf32_max": max(err_x3),
                          "rel_frob_vs_fp64_plain_max": max(err_ff),
@@ -891,6 +929,8 @@ def main():
                     choices=list(WORKLOADS) + ["f32-groups", "serve"])
     ap.add_argument("--group-chains", type=int, default=512,
                     help="f32-groups: chains in the group (fewer: a small case for profiling)")
+    ap.add_argument("--skinny-only", action="store_true",
+                    help="f32-groups: only the tall-skinny chains (a small HBM-bound profiling case)")
     ap.add_argument("--serve-requests", type=int, default=20000,
                     help="serve: Poisson requests per rate point")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[0.3, 0.6, 0.9],

@@ -52,7 +52,7 @@ struct GroupGeo {
     static constexpr int ACC_COLS = BN;
     static constexpr int CORR_COLS = 2 * BN;
     static constexpr int TMEM_COLS = (T::split ? 4 : 2) * BN;
-    static constexpr int STAGING_BYTES = T::split ? 0 : kEpiStagingBytes;
+    static constexpr int STAGING_BYTES = kEpiStagingBytes;
     static constexpr int SMEM_BYTES = S * STAGE_BYTES + STAGING_BYTES + 1024 + 256;
     static constexpr uint32_t idesc = OP == OP_BF16 ? make_idesc(1, 1, 1, 0, 1, kBM, BN)
                                     : OP == OP_I8   ? make_idesc(2, 0, 1, 0, 1, kBM, BN)
@@ -68,6 +68,7 @@ struct alignas(64) GroupStage {
     CUtensorMap tm_w2;   // INT8: the pre-shifted tail block; 3xTF32: weights lo
     CUtensorMap tm_x2;   // 3xTF32: activations lo
     CUtensorMap tm_out;  // output, for the staged (TMA-store) epilogue
+    CUtensorMap tm_out2; // 3xTF32 between stages: the lo half of the output
     StageArgs a;
     int tiles_m, tiles_n;
     int prev;            // stage whose output this one reads (-1: none)
@@ -375,7 +376,58 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
                         cb_ph ^= 1;
                     }
                 }
-                if (ok) {
+                if (ok && cs.a.tma_store) {
+                    // staged TMA stores, 32 columns at a time: the FP32 result, or the
+                    // (hi, lo) TF32 pair of the next stage's input in the two buffers
+                    const int warp_row0 = m0 + quarter * 32;
+                    const bool rows_in = warp_row0 < cs.a.M;
+                    const bool split_out = cs.a.epi == EPI_TF32SPLIT;
+#pragma unroll
+                    for (int c = 0; c < BN / 32; ++c) {
+                        const int nc = n0 + c * 32;
+                        if (nc >= cs.a.N) break;  // warp-uniform
+                        uint8_t *b0 = staging + (split_out ? 0 : sbuf) * kStageBufBytes;
+                        uint8_t *b1 = staging + kStageBufBytes;
+                        if (lane == 0) {
+                            if (split_out)
+                                bulk_wait_read<0>();  // both buffers' last stores have read them
+                            else
+                                bulk_wait_read<1>();
+                        }
+                        __syncwarp();
+                        if (split_out) {
+#pragma unroll
+                            for (int j = 0; j < 8; ++j) {
+                                uint32_t h[4], l[4];
+#pragma unroll
+                                for (int u = 0; u < 4; ++u) {
+                                    const float x = sum[c][4 * j + u];
+                                    const float hf = f32_to_tf32_rne(x);
+                                    h[u] = __float_as_uint(hf);
+                                    l[u] = __float_as_uint(f32_to_tf32_rne(x - hf));
+                                }
+                                st_sw16(b0, lane, 16 * j, make_uint4(h[0], h[1], h[2], h[3]));
+                                st_sw16(b1, lane, 16 * j, make_uint4(l[0], l[1], l[2], l[3]));
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 8; ++j)
+                                st_sw16(b0, lane, 16 * j,
+                                        make_uint4(__float_as_uint(sum[c][4 * j]),
+                                                   __float_as_uint(sum[c][4 * j + 1]),
+                                                   __float_as_uint(sum[c][4 * j + 2]),
+                                                   __float_as_uint(sum[c][4 * j + 3])));
+                            sbuf ^= 1;
+                        }
+                        fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0 && rows_in) {
+                            tma_store_2d(&cs.tm_out, b0, nc, warp_row0);
+                            if (split_out) tma_store_2d(&cs.tm_out2, b1, nc, warp_row0);
+                            bulk_commit();
+                        }
+                    }
+                } else if (ok) {
 #pragma unroll
                     for (int c = 0; c < BN / 32; ++c) {
                         const int nc = n0 + c * 32;
@@ -571,8 +623,19 @@ cudaError_t plan_single(const StageArgs *stages, const int *prev, int n, int ker
                 return cudaErrorInvalidValue;
         }
         cs.a = a;
-        cs.a.tma_store = (!T::split && make_out_map(&cs.tm_out, cs.a)) ? 1 : 0;
-        if (!cs.a.tma_store) cs.tm_out = cs.tm_w;
+        if (a.epi == EPI_TF32SPLIT) {
+            // the next stage's (hi, lo) inputs: FP32 rows of 16-byte multiples
+            const bool ok = ((uintptr_t)a.out & 15) == 0 && ((uintptr_t)a.out_lo & 15) == 0 &&
+                            (a.ld_out * 4) % 16 == 0 &&
+                            make_map(&cs.tm_out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.out, a.M,
+                                     a.N, a.ld_out, 32, 32) &&
+                            make_map(&cs.tm_out2, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.out_lo,
+                                     a.M, a.N, a.ld_out, 32, 32);
+            cs.a.tma_store = ok ? 1 : 0;
+        } else {
+            cs.a.tma_store = make_out_map(&cs.tm_out, cs.a) ? 1 : 0;
+        }
+        if (!cs.a.tma_store) cs.tm_out = cs.tm_out2 = cs.tm_w;
         cs.tiles_m = (a.M + kBM - 1) / kBM;
         cs.tiles_n = (a.N + BN - 1) / BN;
         if (cs.tiles_m > 65535 || cs.tiles_n > 65535) return cudaErrorNotSupported;
