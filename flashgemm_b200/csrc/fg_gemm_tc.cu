@@ -34,7 +34,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     tc_stage_kernel(const __grid_constant__ CUtensorMap tm_w, const __grid_constant__ CUtensorMap tm_x,
                     const __grid_constant__ CUtensorMap tm_w_lo,
                     const __grid_constant__ CUtensorMap tm_x_lo,
-                    const __grid_constant__ CUtensorMap tm_out, const StageArgs p)
+                    const __grid_constant__ CUtensorMap tm_out,
+                    const __grid_constant__ CUtensorMap tm_out2, const StageArgs p)
 {
     using T = OpTraits<OP>;
     using G = Geometry<OP>;
@@ -238,6 +239,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         if constexpr (T::split) {
             int cb = 0;
             uint32_t cb_ph = 0;
+            uint8_t *staging = smem + S * G::STAGE_BYTES + (warp - 2) * 2 * kStageBufBytes;
+            int sbuf = 0;
             for (int t = blockIdx.x; t < num_tiles; t += gridDim.x) {
                 const int m0 = (t / tiles_n) * kBM;
                 const int n0 = (t % tiles_n) * BN;
@@ -297,14 +300,67 @@ __global__ void __launch_bounds__(kThreads, 1)
                     set_abort(bars);
                     break;
                 }
+                if (p.tma_store) {
+                    // staged TMA stores, 32 columns at a time: the FP32 result, or the
+                    // (hi, lo) TF32 pair of the next stage's input in the two buffers
+                    const int warp_row0 = m0 + quarter * 32;
+                    const bool rows_in = warp_row0 < p.M;
+                    const bool split_out = p.epi == EPI_TF32SPLIT;
 #pragma unroll
-                for (int c = 0; c < BN / 32; ++c) {
-                    const int nc = n0 + c * 32;
-                    if (nc < p.N && row < p.M) {
-                        uint32_t v[32];
+                    for (int c = 0; c < BN / 32; ++c) {
+                        const int nc = n0 + c * 32;
+                        if (nc >= p.N) break;  // warp-uniform
+                        uint8_t *b0 = staging + (split_out ? 0 : sbuf) * kStageBufBytes;
+                        uint8_t *b1 = staging + kStageBufBytes;
+                        if (lane == 0) {
+                            if (split_out)
+                                bulk_wait_read<0>();
+                            else
+                                bulk_wait_read<1>();
+                        }
+                        __syncwarp();
+                        if (split_out) {
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) v[j] = __float_as_uint(sum[c][j]);
-                        store_chunk<OP>(p, row, nc, v);
+                            for (int j = 0; j < 8; ++j) {
+                                uint32_t h[4], l[4];
+#pragma unroll
+                                for (int u = 0; u < 4; ++u) {
+                                    const float x = sum[c][4 * j + u];
+                                    const float hf = f32_to_tf32_rne(x);
+                                    h[u] = __float_as_uint(hf);
+                                    l[u] = __float_as_uint(f32_to_tf32_rne(x - hf));
+                                }
+                                st_sw16(b0, lane, 16 * j, make_uint4(h[0], h[1], h[2], h[3]));
+                                st_sw16(b1, lane, 16 * j, make_uint4(l[0], l[1], l[2], l[3]));
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 8; ++j)
+                                st_sw16(b0, lane, 16 * j,
+                                        make_uint4(__float_as_uint(sum[c][4 * j]),
+                                                   __float_as_uint(sum[c][4 * j + 1]),
+                                                   __float_as_uint(sum[c][4 * j + 2]),
+                                                   __float_as_uint(sum[c][4 * j + 3])));
+                            sbuf ^= 1;
+                        }
+                        fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0 && rows_in) {
+                            tma_store_2d(&tm_out, b0, nc, warp_row0);
+                            if (split_out) tma_store_2d(&tm_out2, b1, nc, warp_row0);
+                            bulk_commit();
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < BN / 32; ++c) {
+                        const int nc = n0 + c * 32;
+                        if (nc < p.N && row < p.M) {
+                            uint32_t v[32];
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) v[j] = __float_as_uint(sum[c][j]);
+                            store_chunk<OP>(p, row, nc, v);
+                        }
                     }
                 }
                 if (aborted(bars)) break;
@@ -598,9 +654,22 @@ static cudaError_t launch_op(const StageArgs &a, int num_sms, cudaStream_t s)
     const int grid = tiles < num_sms ? tiles : num_sms;
     StageArgs b = a;
     CUtensorMap to;
-    b.tma_store = (!T::split && make_out_map(&to, b)) ? 1 : 0;
+    CUtensorMap to2;
+    if (b.epi == EPI_TF32SPLIT) {
+        // the next stage's (hi, lo) inputs: FP32 rows of 16-byte multiples
+        const bool ok = ((uintptr_t)b.out & 15) == 0 && ((uintptr_t)b.out_lo & 15) == 0 &&
+                        (b.ld_out * 4) % 16 == 0 &&
+                        make_map(&to, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, b.out, b.M, b.N,
+                                 b.ld_out, 32, 32) &&
+                        make_map(&to2, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, b.out_lo, b.M, b.N,
+                                 b.ld_out, 32, 32);
+        b.tma_store = ok ? 1 : 0;
+    } else {
+        b.tma_store = make_out_map(&to, b) ? 1 : 0;
+    }
     if (!b.tma_store) to = tw;
-    tc_stage_kernel<OP><<<grid, kThreads, G::SMEM_BYTES, s>>>(tw, tx, twl, txl, to, b);
+    if (b.epi != EPI_TF32SPLIT || !b.tma_store) to2 = to;
+    tc_stage_kernel<OP><<<grid, kThreads, G::SMEM_BYTES, s>>>(tw, tx, twl, txl, to, to2, b);
     return cudaGetLastError();
 }
 

@@ -78,7 +78,7 @@ struct Geometry {
     static constexpr int ACC_COLS = T::BN;
     static constexpr int CORR_COLS = 2 * T::BN;
     static constexpr int TMEM_COLS = (T::split ? 4 : 2) * T::BN;
-    static constexpr int STAGING_BYTES = T::split ? 0 : 4 * 2 * 4096;  // TMA-store epilogue
+    static constexpr int STAGING_BYTES = 4 * 2 * 4096;  // TMA-store epilogue, 2 buffers per warp
     static constexpr int SMEM_BYTES =
         T::STAGES * STAGE_BYTES + STAGING_BYTES + 1024 /*align*/ + 256 /*bars*/;
 };
