@@ -99,3 +99,38 @@ def test_settings_round_trip(fg):
     fg.set_semantics("ref")
     assert fg.get_semantics() == fg.FG_SEM_REF
     assert "sm_100a" in fg.version()
+
+
+def test_group_config_round_trip(fg):
+    fg.set_group_config(fg.FG_GROUP_SINGLE_256, fg.FG_ORDER_LEVELS)
+    assert fg.get_group_config() == (fg.FG_GROUP_SINGLE_256, fg.FG_ORDER_LEVELS)
+    fg.set_group_config(7, 9)  # out of range: back to the autotuner's choice
+    assert fg.get_group_config() == (fg.FG_GROUP_AUTO, fg.FG_ORDER_AUTO)
+
+
+def test_autotune_table_file_round_trip(fg, tmp_path):
+    """The remembered (kernel, order) choices survive a save / load; malformed
+    lines and out-of-range choices are skipped. Host-only: no device needed."""
+    src = tmp_path / "in.txt"
+    sig_a = "0/0;256:1024x512,512x1024"
+    sig_b = "1/0;64:64x64"
+    src.write_text(f"0 1 {sig_a}\n2 0 {sig_b}\nnot a line\n5 0 3/0;1:1x1\n")
+    fg.autotune_load(src)
+    out = tmp_path / "out.txt"
+    fg.autotune_save(out)
+    lines = out.read_text().splitlines()
+    assert f"0 1 {sig_a}" in lines and f"2 0 {sig_b}" in lines
+    assert not any("3/0;1:1x1" in l for l in lines)
+    with pytest.raises(fg.FlashgemmError):
+        fg.autotune_load(tmp_path / "missing.txt")
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the no-device path")
+def test_server_and_group_calls_report_no_device(fg):
+    with pytest.raises(fg.FlashgemmError) as e:
+        fg.Server()
+    assert e.value.status == fg.FG_ERR_NO_DEVICE
+    L = fg.lib()
+    import ctypes
+    L.fg_chain_group.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    assert L.fg_chain_group(fg.FG_DT_BF16, 0, None, None) != fg.FG_OK
