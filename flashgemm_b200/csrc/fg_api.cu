@@ -1408,9 +1408,11 @@ size_t group_buf_bytes(int dtype, int algo, int nchains, const fg_chain_desc *ch
 // plus 3 us of launch; fused: max(all work / workers, the longest chain's
 // tiles back to back with 2 us hand-offs). The result is divided by the
 // kernel's efficiency measured on the 512-chain grouped workload relative to
-// the best kernel for that operand type (B200: BF16 pair 1.0, 128x256 0.90,
-// 128x128 0.74; INT8 pair 0.90, 128x256 1.0, 128x128 0.82), and fused runs pay
-// the 8% their dependency waits cost there.
+// the best kernel for that operand type (B200: BF16 pair 0.98, 128x256 1.0,
+// 128x128 0.77; INT8 pair 0.85, 128x256 1.0, 128x128 0.80). Fused runs of the
+// pair kernel, whose CTA pairs follow static lists, pay the 10% their
+// dependency waits cost there; the single-CTA kernel takes its tiles from one
+// list in turn and pays none.
 struct ModelStage {
     long M, N, K;
     int prev, depth;
@@ -1437,8 +1439,8 @@ double model_makespan(int kernel, int order, int op, int sms, const std::vector<
         maxd = std::max(maxd, st[i].depth);
     }
     double eff = 1.0;
-    if (op == OP_BF16) eff = kernel == GK_PAIR ? 1.0 : kernel == GK_SINGLE_256 ? 0.90 : 0.74;
-    if (op == OP_I8) eff = kernel == GK_PAIR ? 0.90 : kernel == GK_SINGLE_256 ? 1.0 : 0.82;
+    if (op == OP_BF16) eff = kernel == GK_PAIR ? 0.98 : kernel == GK_SINGLE_256 ? 1.0 : 0.77;
+    if (op == OP_I8) eff = kernel == GK_PAIR ? 0.85 : kernel == GK_SINGLE_256 ? 1.0 : 0.80;
     double t = 0.0;
     if (order == FG_ORDER_LEVELS) {
         std::vector<double> lw(maxd + 1, 0.0), lt(maxd + 1, 0.0);
@@ -1455,7 +1457,7 @@ double model_makespan(int kernel, int order, int op, int sms, const std::vector<
             path[i] = (st[i].prev >= 0 ? path[st[i].prev] + 2.0 : 0.0) + tile[i];
             crit = std::max(crit, path[i]);
         }
-        t = std::max(1.08 * total / units, crit) + 3.0;
+        t = std::max((pair ? 1.10 : 1.0) * total / units, crit) + 3.0;
     }
     return t / eff;
 }

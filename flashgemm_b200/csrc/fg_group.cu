@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <queue>
@@ -78,10 +79,23 @@ struct alignas(64) GroupStage {
 struct GroupArgs {
     const GroupStage *st;
     const WorkEntry *sched;
-    const int *off;  // CTA c runs sched[off[c] .. off[c + 1])
+    const int *off;  // static lists: CTA c runs sched[off[c] .. off[c + 1])
     int *done;
     int *status;
+    int dynamic;     // 1: one list sched[0 .. total) in dependency order, taken in turn
+    int total;       //    by the CTAs through the counter *next (zeroed with `done`)
+    int *next;
 };
+
+// Entries a CTA's producer has taken, handed in order to its MMA warp and
+// epilogue warps (dynamic lists). Lives in the bytes after Bars.
+constexpr int kRing = 4;
+struct EntryRing {
+    uint64_t full[kRing];   // the producer published entry[slot]
+    uint64_t empty[kRing];  // the MMA warp and the 4 epilogue warps have read it
+    int entry[kRing];       // work entry index, -1: no more work
+};
+static_assert(sizeof(Bars) + sizeof(EntryRing) <= 256, "barrier block");
 
 // Epilogue warps per CTA: counter increments per finished tile.
 constexpr int kGroupDonePerTile = 4;
@@ -100,8 +114,20 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     int *status = g.status;
-    const int q_begin = g.off[blockIdx.x];
-    const int q_end = g.off[blockIdx.x + 1];
+    const int q_begin = g.dynamic ? 0 : g.off[blockIdx.x];
+    const int q_end = g.dynamic ? 0 : g.off[blockIdx.x + 1];
+    EntryRing *ring = reinterpret_cast<EntryRing *>(reinterpret_cast<uint8_t *>(bars) + sizeof(Bars));
+    // k-th entry of this CTA (static list) or of its ring (dynamic): -1 when done,
+    // -2 when a wait ran out
+    auto take = [&](int k, bool release, int code) -> int {
+        if (!g.dynamic) return q_begin + k < q_end ? q_begin + k : -1;
+        const int slot = k % kRing;
+        const uint32_t rph = (uint32_t)(k / kRing) & 1u;
+        if (!mbar_wait(&ring->full[slot], rph, status, code)) return -2;
+        const int q = *reinterpret_cast<volatile int *>(&ring->entry[slot]);
+        if (release) mbar_arrive(&ring->empty[slot]);
+        return q;
+    };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
@@ -117,6 +143,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
                 mbar_init(&bars->full[6 + a], 1);                    // correction ready
                 mbar_init(&bars->empty[6 + a], kGroupDonePerTile);   // correction drained
             }
+        for (int i = 0; i < kRing; ++i) {
+            mbar_init(&ring->full[i], 1);
+            mbar_init(&ring->empty[i], 1 + kGroupDonePerTile);
+        }
         mbar_init(&bars->mma_done, 1);
         bars->abort = 0;
         fence_mbar_init();
@@ -134,7 +164,25 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
             uint32_t ph = 0;
             uint32_t pending = 0, pending_ph = 0;
             int last_si = -1;
-            for (int q = q_begin; q < q_end; ++q) {
+            for (int k = 0;; ++k) {
+                int q;
+                if (g.dynamic) {
+                    // take the next entry of the global list and publish it to this
+                    // CTA's MMA and epilogue warps
+                    const int slot = k % kRing;
+                    const uint32_t rph = (uint32_t)(k / kRing) & 1u;
+                    if (!mbar_wait(&ring->empty[slot], rph ^ 1, status, KERR_WAIT_EMPTY)) {
+                        set_abort(bars);
+                        goto producer_done;
+                    }
+                    q = atomicAdd(g.next, 1);
+                    if (q >= g.total) q = -1;
+                    *reinterpret_cast<volatile int *>(&ring->entry[slot]) = q;
+                    mbar_arrive(&ring->full[slot]);
+                } else {
+                    q = q_begin + k < q_end ? q_begin + k : -1;
+                }
+                if (q < 0) break;
                 const WorkEntry e = g.sched[q];
                 const int si = (int)e.stage;
                 const int mb = (int)(e.mbnb >> 16), nb = (int)(e.mbnb & 0xffffu);
@@ -225,7 +273,13 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
             uint32_t acc_ph = 0;
             int cb = 0;          // 3xTF32: correction accumulator of this tile
             uint32_t cb_ph = 0;
-            for (int q = q_begin; q < q_end; ++q) {
+            for (int k = 0;; ++k) {
+                const int q = take(k, true, KERR_WAIT_FULL);
+                if (q == -2) {
+                    set_abort(bars);
+                    goto mma_done;
+                }
+                if (q < 0) break;
                 const GroupStage &cs = g.st[g.sched[q].stage];
                 const int num_kb = (cs.a.K + G::BK - 1) / G::BK;
                 // 3xTF32 hands the hi*hi partial sum to the epilogue every kchunk
@@ -313,7 +367,17 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
         uint32_t cb_ph = 0;
         uint8_t *staging = smem + S * G::STAGE_BYTES + (warp - 2) * 2 * kStageBufBytes;
         int sbuf = 0;
-        for (int q = q_begin; q < q_end; ++q) {
+        for (int k = 0;; ++k) {
+            const int q = take(k, false, KERR_WAIT_ACC_FULL);
+            if (g.dynamic) {
+                __syncwarp();
+                if (lane == 0 && q != -2) mbar_arrive(&ring->empty[k % kRing]);
+            }
+            if (q == -2) {
+                set_abort(bars);
+                break;
+            }
+            if (q < 0) break;
             const WorkEntry e = g.sched[q];
             const int mb = (int)(e.mbnb >> 16), nb = (int)(e.mbnb & 0xffffu);
             const GroupStage &cs = g.st[e.stage];
@@ -489,7 +553,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
 // ------------------------------------------------------------------ scheduling (host)
 
 void list_schedule(const SchedStage *st, int n, int units, double handoff, std::vector<int> &off,
-                   std::vector<WorkEntry> &entries, double *makespan)
+                   std::vector<WorkEntry> &entries, double *makespan, std::vector<double> *starts)
 {
     double span = 0.0;
     std::vector<int> depth(n, 0), order(n);
@@ -503,6 +567,7 @@ void list_schedule(const SchedStage *st, int n, int units, double handoff, std::
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return depth[x] < depth[y]; });
     std::vector<double> block_done(nblocks, 0.0);
     std::vector<std::vector<WorkEntry>> per(units);
+    std::vector<std::vector<double>> per_start(starts ? units : 0);
     // Small problems (one chain's few hundred tiles): scan every worker, ties to
     // the lowest index. Larger ones: a heap of (free time, worker), O(log workers)
     // per tile; a tile whose input is not ready before the earliest free worker
@@ -538,6 +603,7 @@ void list_schedule(const SchedStage *st, int n, int units, double handoff, std::
                 else
                     heap.push({fin, best});
                 per[best].push_back(WorkEntry{(uint32_t)si, ((uint32_t)mb << 16) | (uint32_t)nb});
+                if (starts) per_start[best].push_back(start);
                 double &bd = block_done[c.done_off + nb];
                 if (fin > bd) bd = fin;
                 if (fin > span) span = fin;
@@ -547,15 +613,27 @@ void list_schedule(const SchedStage *st, int n, int units, double handoff, std::
     off.assign(units + 1, 0);
     entries.clear();
     entries.reserve(total);
+    if (starts) starts->clear();
     for (int u = 0; u < units; ++u) {
         off[u + 1] = off[u] + (int)per[u].size();
         entries.insert(entries.end(), per[u].begin(), per[u].end());
+        if (starts) starts->insert(starts->end(), per_start[u].begin(), per_start[u].end());
     }
 }
 
 // ------------------------------------------------------------------ planning and launch (host)
 
 namespace {
+
+// Dynamic lists for the single-CTA kernel (FG_GROUP_DYNAMIC=0: static per-CTA lists).
+bool group_dynamic()
+{
+    static const bool on = [] {
+        const char *v = getenv("FG_GROUP_DYNAMIC");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
 
 template <int OP, int BN, int S>
 cudaError_t single_capacity(int num_sms, int &ctas)
@@ -653,13 +731,29 @@ cudaError_t plan_single(const StageArgs *stages, const int *prev, int n, int ker
     if (items < ctas) ctas = (int)items;
     std::vector<int> off;
     std::vector<WorkEntry> ent;
-    list_schedule(ss.data(), n, ctas, 2.0, off, ent);
+    std::vector<double> starts;
+    const bool dyn = group_dynamic();
+    list_schedule(ss.data(), n, ctas, 2.0, off, ent, nullptr, dyn ? &starts : nullptr);
+    if (dyn) {
+        // one list in order of the schedule's start times (every dependency
+        // starts earlier, so it comes first), taken by the CTAs in turn
+        std::vector<int> order(ent.size());
+        for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int x, int y) { return starts[x] < starts[y]; });
+        std::vector<WorkEntry> sorted(ent.size());
+        for (size_t i = 0; i < order.size(); ++i) sorted[i] = ent[order[i]];
+        ent.swap(sorted);
+        off.assign(ctas + 1, (int)items);
+        off[0] = 0;
+    }
     auto r = [](size_t b) { return (b + 255) & ~(size_t)255; };
     out.kernel = kernel;
     out.op = OP;
     out.ctas = ctas;
     out.entries = items;
-    out.done_ints = (size_t)done_off;
+    out.dynamic = dyn ? 1 : 0;
+    out.done_ints = (size_t)done_off + 1;  // the last one: the dynamic list's counter
     out.off_st = 0;
     out.off_sched = r((size_t)n * sizeof(GroupStage));
     out.off_off = out.off_sched + r((size_t)items * sizeof(WorkEntry));
@@ -682,6 +776,9 @@ cudaError_t launch_single(const GroupLaunch &g, const void *tables_dev, int *don
     a.off = reinterpret_cast<const int *>(base + g.off_off);
     a.done = done;
     a.status = status;
+    a.dynamic = g.dynamic;
+    a.total = (int)g.entries;
+    a.next = done + g.done_ints - 1;
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;  // all CTAs resident: they wait on one another

@@ -86,8 +86,10 @@ struct SchedStage {
 // Worker u runs entries[off[u] .. off[u+1]) in that order, so the earliest
 // unfinished entry always heads its worker's list and no worker waits forever.
 // makespan (optional): the estimated finish time of the last tile.
+// starts (optional): each entry's estimated start, in the order of `entries`.
 void list_schedule(const SchedStage *st, int n, int units, double handoff, std::vector<int> &off,
-                   std::vector<WorkEntry> &entries, double *makespan = nullptr);
+                   std::vector<WorkEntry> &entries, double *makespan = nullptr,
+                   std::vector<double> *starts = nullptr);
 
 enum GroupKernel : int {
     GK_PAIR = 0,        // BF16 / INT8: CTA pairs, 256 x 256 tiles, 6-stage ring
@@ -104,6 +106,7 @@ struct GroupLaunch {
     int ctas = 0;             // CTAs launched (pairs x 2 for GK_PAIR)
     long entries = 0;         // tiles
     size_t done_ints = 0;     // zeroed counters the launch needs
+    int dynamic = 0;          // single-CTA kernel: one list taken in turn (counter: last int)
     size_t off_st = 0, off_sched = 0, off_off = 0;  // table offsets in `tables`
     std::vector<unsigned char> tables;
 };
