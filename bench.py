@@ -1068,6 +1068,44 @@ def main():
         fg.set_chain_mode("fused")
         per_gemm = (pg_ms, pg_launches)
 
+    # a plain library path beside it: one cuBLAS GEMM per stage (torch), the
+    # narrowing between stages as separate kernels, intermediates in HBM (same
+    # shapes and dtypes; INT8 with signed weights, cuBLAS having no unsigned x
+    # signed GEMM; no panel permutation)
+    cublas = None
+    if dt != "f32":
+        if dt == "bf16":
+            cA = [a.view(torch.bfloat16) for a in tA]
+            cB = tB.view(torch.bfloat16)
+
+            def plain():
+                x = cB
+                for a in cA:
+                    x = a @ x  # FP32 accumulation, BF16 result (RNE)
+                return x.float()
+        else:
+            cA = list(tA)
+            cB = tB
+
+            def plain():
+                x = cB
+                for i, a in enumerate(cA):
+                    y = torch._int_mm(a, x)
+                    x = y if i == len(cA) - 1 else y.clamp_(-128, 127).to(torch.int8)
+                return x
+        for _ in range(max(args.warmup, 3)):
+            plain()
+        torch.cuda.synchronize(dev)
+        cs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ce = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        for i in range(args.steps):
+            flush.fill_(i & 0xFF)
+            cs[i].record()
+            plain()
+            ce[i].record()
+        torch.cuda.synchronize(dev)
+        cublas = sum(a.elapsed_time(b) for a, b in zip(cs, ce))
+
     # max over ranks
     if dist:
         t = torch.tensor([total_ms, per_gemm[0] if per_gemm else 0.0], dtype=torch.float64,
@@ -1163,6 +1201,13 @@ def main():
                             "launches": per_gemm[1],
                             "path": "one tensor-core launch per GEMM (FG_CHAIN_PER_GEMM)"}
         line["fused_vs_per_gemm"] = value / pg_value
+    if cublas:
+        cb_value = world * step_flops * args.steps / (cublas / 1e3) / 1e12
+        line["cublas_per_gemm"] = {
+            "value": cb_value, "unit": "TFLOP/s", "ms_per_step": cublas / args.steps,
+            "path": "torch.matmul / torch._int_mm (cuBLAS) per GEMM, narrowing as separate "
+                    "kernels, intermediates in HBM; INT8 with signed weights, no panel permutation"}
+        line["fused_vs_cublas_per_gemm"] = value / cb_value
     if world == 1:
         tf, descr, _ = time_cpu(args.workload, budget_s=args.cpu_budget)
         line["cpu_baseline"] = dict(descr, value=tf, unit="TFLOP/s")
