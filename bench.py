@@ -870,9 +870,17 @@ def run_serve(args, world, rank, local_rank):
     for ws in W:
         for w in ws:
             w.release()
+    # whole job: throughput summed over the ranks' streams, latency the worst rank's
+    job_tflops = points[-1]["tflops"]
+    job_e2e = st_e2e["flops"] / st_e2e["span_s"] / 1e12
+    lat = [points[-1]["p50_us"], points[-1]["p99_us"]]
     if dist:
-        t = torch.tensor([points[-1]["tflops"]], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        t = torch.tensor([job_tflops, job_e2e], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        job_tflops, job_e2e = float(t[0].item()), float(t[1].item())
+        t = torch.tensor(lat, dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        lat = [float(x) for x in t.tolist()]
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
@@ -894,15 +902,15 @@ def run_serve(args, world, rank, local_rank):
                     "peak_source": ("bf16_tflops" if name == "bf16" else
                                     "2 x bf16_tflops" if name == "int8" else
                                     "bf16_tflops / 2 / 3") + f"; {peak_src}"}
-    line = {"metric": metric, "value": world * top["tflops"], "unit": "TFLOP/s", "n_gpus": world,
+    line = {"metric": metric, "value": job_tflops, "unit": "TFLOP/s", "n_gpus": world,
             "steps": len(points), "warmup": 1, "ms_per_step": None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "bf16/int8/f32(3xTF32) mix",
             "data": "synthetic (seeded; no dataset involved)", "config": config,
             "clocks": sampler.summary(), "gpu_launches": launches_total,
-            "latency": {"p50_us": top["p50_us"], "p99_us": top["p99_us"],
+            "latency": {"p50_us": lat[0], "p99_us": lat[1], "ranks": "worst rank",
                         "at_offered_frac_of_capacity": top["offered_frac_of_capacity"]},
             "capacity_req_s": capacity, "points": points,
-            "e2e": {"value": st_e2e["flops"] / st_e2e["span_s"] / 1e12 * world, "unit": "TFLOP/s",
+            "e2e": {"value": job_e2e, "unit": "TFLOP/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "step": f"{e2e_n} requests at 0.6 x capacity",
                     "p50_us": st_e2e["p50_us"], "p99_us": st_e2e["p99_us"],
