@@ -229,7 +229,7 @@ size_t chain_scratch(int dtype, int algo, long N, int n, const long *M, const lo
     long maxM = 0;
     for (int i = 0; i < n - 1; ++i) maxM = M[i] > maxM ? M[i] : maxM;
     if (dtype == FG_DT_INT8 || dtype == FG_DT_BF16) {  // fused-chain completion counters
-        s += carve_size((size_t)n * ((N + 255) / 256) * sizeof(int));
+        s += carve_size(chain_counter_ints(n, M, N) * sizeof(int));
         if (getenv("FG_TRACE_DIR")) {  // per-tile timeline of the fused kernel
             size_t items = 0;
             for (int i = 0; i < n; ++i) items += (size_t)((M[i] + 255) / 256) * ((N + 255) / 256);
@@ -285,8 +285,11 @@ int launch_stages(DevCtx *c, int kind, std::vector<StageArgs> &stages, long N)
     const int n = (int)stages.size();
     if (fused_enabled() && n <= chain_max_stages() && !g_fused_unsupported[c->dev & 63]) {
         const long tiles_n = (N + 255) / 256;
-        int *done = (int *)arena_take(c, (size_t)n * tiles_n * sizeof(int));
-        CUDA_TRY(cudaMemsetAsync(done, 0, (size_t)n * tiles_n * sizeof(int), c->stream));
+        std::vector<long> rows(n);
+        for (int i = 0; i < n; ++i) rows[i] = stages[i].M;
+        const size_t done_ints = chain_counter_ints(n, rows.data(), N);
+        int *done = (int *)arena_take(c, done_ints * sizeof(int));
+        CUDA_TRY(cudaMemsetAsync(done, 0, done_ints * sizeof(int), c->stream));
         double fl = 0.0;
         for (auto &st : stages) fl += gemm_flops(st.M, st.N, st.K);
         // FG_TRACE_DIR=<dir>: write a per-tile timeline of every fused launch there

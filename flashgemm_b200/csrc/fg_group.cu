@@ -562,7 +562,8 @@ void list_schedule(const SchedStage *st, int n, int units, double handoff, std::
         depth[i] = st[i].prev < 0 ? 0 : depth[st[i].prev] + 1;
         order[i] = i;
         total += (long)st[i].tiles_m * st[i].tiles_n;
-        nblocks = std::max<long>(nblocks, (long)st[i].done_off + st[i].tiles_n);
+        nblocks = std::max<long>(nblocks, (long)st[i].done_off +
+                                              (long)st[i].tiles_n * (st[i].row_done ? st[i].tiles_m : 1));
     }
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return depth[x] < depth[y]; });
     std::vector<double> block_done(nblocks, 0.0);
@@ -580,9 +581,21 @@ void list_schedule(const SchedStage *st, int n, int units, double handoff, std::
         for (int u = 0; u < units; ++u) heap.push({0.0, u});
     for (int si : order) {
         const SchedStage &c = st[si];
-        for (int nb = 0; nb < c.tiles_n; ++nb)
-            for (int mb = 0; mb < c.tiles_m; ++mb) {
-                const double ready = c.prev >= 0 ? block_done[st[c.prev].done_off + nb] + handoff : 0.0;
+        const long count = (long)c.tiles_m * c.tiles_n;
+        for (long it = 0; it < count; ++it) {
+            const int nb = (int)(c.row_major ? it % c.tiles_n : it / c.tiles_m);
+            const int mb = (int)(c.row_major ? it / c.tiles_n : it % c.tiles_m);
+                double ready = 0.0;
+                if (c.prev >= 0) {
+                    const SchedStage &p = st[c.prev];
+                    if (!p.row_done) {
+                        ready = block_done[p.done_off + nb] + handoff;
+                    } else {
+                        const double *rd = &block_done[p.done_off + (long)nb * p.tiles_m];
+                        for (int g = 0; g < p.tiles_m; ++g)
+                            ready = std::max(ready, rd[g] + handoff - (c.stream > 0 ? g * c.stream : 0.0));
+                    }
+                }
                 int best = 0;
                 double start;
                 if (scan) {
@@ -604,7 +617,7 @@ void list_schedule(const SchedStage *st, int n, int units, double handoff, std::
                     heap.push({fin, best});
                 per[best].push_back(WorkEntry{(uint32_t)si, ((uint32_t)mb << 16) | (uint32_t)nb});
                 if (starts) per_start[best].push_back(start);
-                double &bd = block_done[c.done_off + nb];
+                double &bd = block_done[c.done_off + (c.row_done ? (long)nb * c.tiles_m + mb : nb)];
                 if (fin > bd) bd = fin;
                 if (fin > span) span = fin;
             }

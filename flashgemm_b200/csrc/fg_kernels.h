@@ -50,13 +50,15 @@ struct StageArgs {
 cudaError_t launch_tc_stage(const StageArgs &a, int num_sms, cudaStream_t s);
 
 // A whole BF16 or INT8 chain (stages[0..n) with the same op and N) in one
-// cooperative persistent launch; `done` holds n * ceil(N / 256) zeroed ints.
+// persistent launch; `done` holds chain_counter_ints() zeroed ints.
 // Returns cudaErrorNotSupported (nothing launched) where the device cannot
 // run it; the caller then launches the stages one by one.
 // trace (optional, else null): chain_trace_fields() %globaltimer stamps per (item, CTA).
 cudaError_t launch_tc_chain(const StageArgs *stages, int n, int *done, int *status,
                             unsigned long long *trace, int num_sms, cudaStream_t s);
 int chain_max_stages();
+// Counters a fused chain of these row counts (n stages, N columns) may use.
+size_t chain_counter_ints(int n, const long *M, long N);
 int chain_trace_fields();
 
 // ------------------------------------------------------------------ grouped launches
@@ -76,13 +78,19 @@ struct WorkEntry {
 struct SchedStage {
     int tiles_m, tiles_n;  // tiles of the stage along M and N
     int prev;              // stage it reads (-1: none), earlier in the list
-    int done_off;          // its first column-block counter
+    int done_off;          // its first counter
     double cost;           // estimated duration of one tile (any unit)
+    int row_done = 0;      // 1: done per (column block, row tile) at done_off + nb * tiles_m + mb
+    int row_major = 0;     // 1: list the stage's tiles row tile by row tile
+    double stream = 0.0;   // > 0: input row tile g is needed only `g * stream` after the
+                           // tile starts (the previous stage has row_done)
 };
 
 // List schedule: stages in dependency depth order, each stage's tiles column
-// block by column block; a tile goes to the worker that can start it first (the
-// worker is free and the column block it reads is estimated done + handoff).
+// block by column block (or row tile by row tile); a tile goes to the worker
+// that can start it first (the worker is free and the column block it reads is
+// estimated done + handoff, or, streaming, each row tile of it is done by the
+// time the tile's k-loop reaches it).
 // Worker u runs entries[off[u] .. off[u+1]) in that order, so the earliest
 // unfinished entry always heads its worker's list and no worker waits forever.
 // makespan (optional): the estimated finish time of the last tile.

@@ -297,6 +297,52 @@ def test_fused_chain_equals_per_gemm_path(fg, dt):
     assert_parity(dt, b, want, (Ms[-1] // 4) * 4 if dt == "int8" else None)
 
 
+_STREAM_SCRIPT = """
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import flashgemm_b200 as fg, oracle
+dt, out = sys.argv[2], sys.argv[3]
+N, K1, Ms = 768, 256, [1000, 520, 136, 300]
+B, As, Ks = oracle.chain_inputs(dt, N, K1, Ms, seed=43)
+fg.set_semantics("ref")
+C = np.zeros((Ms[-1], N), np.int32 if dt == "int8" else np.float32)
+args = []
+for a, m, k in zip(As, Ms, Ks):
+    args += [a, m, k]
+getattr(fg, {"int8": "flashgemm_multi_int8uint8int32",
+             "bf16": "flashgemm_multi_bf16bf16f32"}[dt])(C, B, N, len(Ms), *args, check=True)
+fg.sync()
+np.save(out, C)
+"""
+
+
+@pytest.mark.parametrize("dt", ["int8", "bf16"])
+def test_streamed_hand_off_is_bit_identical(dt, tmp_path):
+    """The streamed hand-off between stages (a stage's tile waits for each
+    256-row tile of its input as its k-loop reaches it) changes only when tiles
+    start, not their arithmetic: forced on and forced off, the fused chain gives
+    identical bits, here with stage K not a multiple of 256 and INT8 tail rows."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = {}
+    for mode in ("0", "1"):
+        path = str(tmp_path / f"c{mode}.npy")
+        env = dict(os.environ, FG_CHAIN_STREAM=mode,
+                   PYTHONPATH=os.pathsep.join([root, os.path.join(root, "oracle")]))
+        r = subprocess.run([sys.executable, "-c", _STREAM_SCRIPT, root, dt, path], env=env,
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout + r.stderr
+        outs[mode] = np.load(path)
+    np.testing.assert_array_equal(outs["0"], outs["1"])
+    N, K1, Ms = 768, 256, [1000, 520, 136, 300]
+    B, As, Ks = oracle.chain_inputs(dt, N, K1, Ms, seed=43)
+    want = oracle.chain(dt, B, As, N, Ms, Ks, mode=oracle.REF, threads=1)
+    assert_parity(dt, outs["1"], want, (Ms[-1] // 4) * 4 if dt == "int8" else None)
+
+
 @pytest.mark.parametrize("dt,f32algo", [("int8", None), ("bf16", None), ("f32", "ffma"),
                                         ("f32", "3xtf32")])
 def test_registered_weights_match_per_call_weights(fg, dt, f32algo):
