@@ -319,11 +319,15 @@ __device__ __forceinline__ uint32_t pack_bf16x2(uint32_t a, uint32_t b)
     return r;
 }
 
+// Four int32 to packed saturated int8 (a in the low byte): two
+// cvt.pack.sat.s8.s32.b32, each of which saturates two values into the low 16
+// bits of its result and copies the low 16 bits of its third operand above them.
 __device__ __forceinline__ uint32_t pack_s8x4(uint32_t a, uint32_t b, uint32_t c, uint32_t d)
 {
-    return (uint32_t)(uint8_t)sat_s8((int32_t)a) | ((uint32_t)(uint8_t)sat_s8((int32_t)b) << 8) |
-           ((uint32_t)(uint8_t)sat_s8((int32_t)c) << 16) |
-           ((uint32_t)(uint8_t)sat_s8((int32_t)d) << 24);
+    uint32_t hi, r;
+    asm("cvt.pack.sat.s8.s32.b32 %0, %1, %2, %3;" : "=r"(hi) : "r"(d), "r"(c), "r"(0u));
+    asm("cvt.pack.sat.s8.s32.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(b), "r"(a), "r"(hi));
+    return r;
 }
 
 // Write TMEM chunk `cc` (32 columns, this lane's row r) of a staging buffer.
