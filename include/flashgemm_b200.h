@@ -61,7 +61,10 @@ int fg_get_sgemm_algo(void);
 
 /* How BF16 / INT8 chains are launched.
  * FG_CHAIN_FUSED (default): the whole chain in one persistent launch; a stage
- *   starts on a 256-column block as soon as the previous stage has stored it.
+ *   starts on a 256-column block as soon as the previous stage has stored it
+ *   (or, where the library's schedule estimate prefers it, streams: it loads
+ *   each 256-row tile of its input once that tile is stored; FG_CHAIN_STREAM=0
+ *   or 1 forces either; the arithmetic and the results are the same).
  * FG_CHAIN_PER_GEMM: one tensor-core launch per GEMM, the plain per-GEMM path
  *   (same kernels' arithmetic, so the same results).
  * The environment variable FG_FUSED=0 selects the per-GEMM path initially. */
