@@ -531,29 +531,33 @@ std::vector<SchedStage> sched_stages(const std::vector<ChainStage> &st, int bk)
     return ss;
 }
 
-// Counter layout of a chain: streaming gives every stage but the last a
-// counter per (column block, row tile).
-void set_counters(std::vector<ChainStage> &st, bool stream)
+// Counter layout of a chain: bit i of `stream` gives stage i (not the last) a
+// counter per (column block, row tile), so that stage i + 1 streams.
+void set_counters(std::vector<ChainStage> &st, unsigned stream)
 {
     int done_off = 0;
     const int n = (int)st.size();
     for (int i = 0; i < n; ++i) {
-        st[i].row_counters = stream && i + 1 < n ? 1 : 0;
+        st[i].row_counters = ((stream >> i) & 1u) && i + 1 < n ? 1 : 0;
         st[i].done_off = done_off;
         done_off += st[i].tiles_n * (st[i].row_counters ? st[i].tiles_m : 1);
     }
 }
 
-// FG_CHAIN_STREAM: 0 = never stream, 1 = always, unset = when the schedule
-// estimate is at least 1 % shorter. (Measured on B200: the BF16 chain
-// 4096x1024 -> 4096 -> 1024 -> 1024, estimate 0.978 of block-wise, ran 4 %
-// faster streamed; the INT8 chain 8192x2048 -> 4096 -> 2048 -> 4096 -> 1024,
-// estimate 1.008, 15 % slower.)
-int stream_mode()
+// FG_CHAIN_STREAM: 0 = never stream, 1 = every stage boundary, m<bits> = the
+// boundaries whose bits are set (bit i: stage i + 1 streams from stage i),
+// unset = every boundary when the schedule estimate is at least 1 % shorter,
+// else none. (Measured on B200: the BF16 chain 4096x1024 -> 4096 -> 1024 ->
+// 1024, estimate 0.978 of block-wise, ran 4 % faster streamed; the INT8 chain
+// 8192x2048 -> 4096 -> 2048 -> 4096 -> 1024, estimate 1.008, 15 % slower.)
+constexpr unsigned kStreamAuto = ~0u;
+unsigned stream_mode()
 {
-    static const int m = [] {
+    static const unsigned m = [] {
         const char *v = getenv("FG_CHAIN_STREAM");
-        return v ? (v[0] == '1' ? 1 : 0) : -1;
+        if (!v) return kStreamAuto;
+        if (v[0] == 'm') return (unsigned)strtoul(v + 1, nullptr, 10) & 0xffu;
+        return v[0] == '1' ? 0xffu : 0u;
     }();
     return m;
 }
@@ -592,7 +596,7 @@ static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, in
     // the schedule depends only on the shapes: computed once per shape set
     struct Cached {
         std::vector<long> key;
-        bool stream;
+        unsigned stream;  // stage boundaries that stream
         std::vector<int> off;
         std::vector<uint32_t> items;
     };
@@ -614,14 +618,16 @@ static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, in
         double span_block = 0.0, span_stream = 0.0;
         std::vector<int> off_s;
         std::vector<WorkEntry> ent_s;
-        set_counters(st, false);
+        set_counters(st, 0u);
         list_schedule(sched_stages(st, G::BK).data(), n, pairs, 2.0, c.off, ent, &span_block);
-        c.stream = false;
-        if (n > 1 && stream_mode() != 0) {
-            set_counters(st, true);
+        c.stream = 0u;
+        const unsigned mode = stream_mode();
+        if (n > 1 && mode != 0u) {
+            const unsigned mask = mode == kStreamAuto ? 0xffu : mode;
+            set_counters(st, mask);
             list_schedule(sched_stages(st, G::BK).data(), n, pairs, 2.0, off_s, ent_s, &span_stream);
-            if (stream_mode() == 1 || span_stream < 0.99 * span_block) {
-                c.stream = true;
+            if (mode != kStreamAuto || span_stream < 0.99 * span_block) {
+                c.stream = mask;
                 c.off.swap(off_s);
                 ent.swap(ent_s);
             }
