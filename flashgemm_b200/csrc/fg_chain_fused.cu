@@ -247,23 +247,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
                 int rows_ready = 0;  // streaming: input row tiles known stored
                 for (int kb = 0; kb < num_kb; ++kb) {
                     if (row_cnt && (kb * G::BK) / 256 >= rows_ready && rows_ready < row_tiles) {
-                        // first k-block of input row tile g: read up to 8 row-tile
-                        // counters from g in one round trip (relaxed loads), wait
-                        // for g itself if it is not stored yet, then take every
-                        // tile of the complete prefix with one acquire
+                        // first k-block of input row tile g: wait until it is stored
                         const int g = min((kb * G::BK) / 256, row_tiles - 1);
-                        int c[8];
-#pragma unroll
-                        for (int j = 0; j < 8; ++j)
-                            c[j] = g + j < row_tiles ? ld_relaxed_gpu(row_cnt + g + j)
-                                                     : 0;
-                        int ready = 0;
-#pragma unroll
-                        for (int j = 0; j < 8; ++j)
-                            if (ready == j && c[j] >= kDoneIncrementsPerTile) ready = j + 1;
-                        if (ready == 0) {
+                        if (ld_acquire_gpu(row_cnt + g) < kDoneIncrementsPerTile) {
                             const uint64_t t0 = globaltimer_ns();
-                            while (ld_relaxed_gpu(row_cnt + g) < kDoneIncrementsPerTile) {
+                            while (ld_acquire_gpu(row_cnt + g) < kDoneIncrementsPerTile) {
                                 __nanosleep(32);
                                 if (globaltimer_ns() - t0 > kWaitLimitNs) {
                                     atomicCAS(status, 0, KERR_WAIT_DEPENDENCY);
@@ -271,11 +259,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
                                     goto producer_done;
                                 }
                             }
-                            ready = 1;
                         }
-                        fence_acquire_gpu();
                         fence_proxy_async_global();
-                        rows_ready = g + ready;
+                        rows_ready = g + 1;
                     }
                     if (!mbar_wait(&bars->empty[s], ph ^ 1, status, KERR_WAIT_EMPTY)) {
                         set_abort(bars);

@@ -376,16 +376,6 @@ __device__ __forceinline__ int ld_acquire_gpu(const int *p)
     return v;
 }
 
-__device__ __forceinline__ int ld_relaxed_gpu(const int *p)
-{
-    int v;
-    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// Acquire side of a relaxed load: orders everything after it behind the loads before it.
-__device__ __forceinline__ void fence_acquire_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
-
 __device__ __forceinline__ void red_release_gpu_add(int *p, int v)
 {
     asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
