@@ -145,6 +145,12 @@ int get_ctx(DevCtx **out)
         CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
         CUDA_TRY(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
         CUDA_TRY(cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming));
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->stream_h2d, cudaStreamNonBlocking));
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->stream_d2h, cudaStreamNonBlocking));
+        for (int j = 0; j < DevCtx::kCopyChunks; ++j) {
+            CUDA_TRY(cudaEventCreateWithFlags(&c->ev_up[j], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&c->ev_done[j], cudaEventDisableTiming));
+        }
         CUDA_TRY(cudaMalloc(&c->status, sizeof(int)));
         CUDA_TRY(cudaMemset(c->status, 0, sizeof(int)));
         CUDA_TRY(cudaMallocHost(&c->status_host, sizeof(int)));
@@ -645,25 +651,74 @@ int host_chain(int dtype, void *C, const void *B, long N, int n, const void *con
     if ((st = arena_reserve(c, need))) return st;
 
     void *bd = arena_take(c, (size_t)K[0] * ldN * elt);
-    CUDA_TRY(cudaMemcpy2DAsync(bd, ldN * elt, B, N * elt, N * elt, K[0], cudaMemcpyHostToDevice,
-                               c->stream));
     std::vector<Mat> ad(n);
+    std::vector<void *> wd(n);
     for (int i = 0; i < n; ++i) {
-        void *p = arena_take(c, (size_t)M[i] * lda[i] * elt);
-        CUDA_TRY(cudaMemcpy2DAsync(p, lda[i] * elt, A[i], K[i] * elt, K[i] * elt, M[i],
-                                   cudaMemcpyHostToDevice, c->stream));
-        ad[i] = Mat{p, lda[i]};
+        wd[i] = arena_take(c, (size_t)M[i] * lda[i] * elt);
+        ad[i] = Mat{wd[i], lda[i]};
     }
     void *cd = arena_take(c, (size_t)M[n - 1] * ldN * out_elt);
-    if ((st = run_chain(c, dtype, sem, algo, cd, ldN, Mat{bd, ldN}, N, n, ad.data(), M, K)))
-        return st;
     // INT8 reference semantics leave rows >= 4 * floor(M / 4) of C untouched
     // (multigemm/src/kernel_int8.h:943-945)
     long rows = M[n - 1];
     if (dtype == FG_DT_INT8 && sem == FG_SEM_REF) rows = (rows / 4) * 4;
-    if (rows > 0)
-        CUDA_TRY(cudaMemcpy2DAsync(C, N * out_elt, cd, ldN * out_elt, N * out_elt, rows,
-                                   cudaMemcpyDeviceToHost, c->stream));
+
+    // Column chunks (fused BF16 / INT8 chains from 1024 columns): the weights and
+    // then each chunk of B go up on one copy stream, each chunk's chain runs on the
+    // compute stream once its columns are there, and its columns of C come back on
+    // a second copy stream while later chunks compute. Chunks start on multiples
+    // of 256 columns: every tile, panel and result is the one of the whole chain.
+    const bool chunked = (dtype == FG_DT_BF16 || dtype == FG_DT_INT8) && fused_enabled() &&
+                         N >= 1024;
+    const int nchunk = chunked ? DevCtx::kCopyChunks : 1;
+    const long cw = chunked ? round_up((N + nchunk - 1) / nchunk, 256) : N;
+    auto drain = [&] {  // no copy may still touch the caller's buffers after a failure
+        cudaStreamSynchronize(c->stream_h2d);
+        cudaStreamSynchronize(c->stream);
+        cudaStreamSynchronize(c->stream_d2h);
+    };
+    for (int i = 0; i < n; ++i) {
+        const cudaError_t e = cudaMemcpy2DAsync(wd[i], lda[i] * elt, A[i], K[i] * elt,
+                                                K[i] * elt, M[i], cudaMemcpyHostToDevice,
+                                                c->stream_h2d);
+        if (e != cudaSuccess) {
+            drain();
+            return fail(FG_ERR_CUDA, "chain upload: %s", cudaGetErrorString(e));
+        }
+    }
+    const size_t mark = c->arena_off;
+    for (int j = 0; j < nchunk; ++j) {
+        const long c0 = j * cw, c1 = c0 + cw < N ? c0 + cw : N;
+        if (c0 >= N) break;
+        char *bj = static_cast<char *>(bd) + c0 * elt;
+        char *cj = static_cast<char *>(cd) + c0 * out_elt;
+        cudaError_t e = cudaMemcpy2DAsync(bj, ldN * elt, static_cast<const char *>(B) + c0 * elt,
+                                          N * elt, (c1 - c0) * elt, K[0], cudaMemcpyHostToDevice,
+                                          c->stream_h2d);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev_up[j], c->stream_h2d);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_up[j], 0);
+        if (e != cudaSuccess) {
+            drain();
+            return fail(FG_ERR_CUDA, "chain upload: %s", cudaGetErrorString(e));
+        }
+        c->arena_off = mark;  // chunks reuse the scratch in stream order
+        if ((st = run_chain(c, dtype, sem, algo, cj, ldN, Mat{bj, ldN}, c1 - c0, n, ad.data(),
+                            M, K))) {
+            drain();
+            return st;
+        }
+        e = cudaEventRecord(c->ev_done[j], c->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream_d2h, c->ev_done[j], 0);
+        if (e == cudaSuccess && rows > 0)
+            e = cudaMemcpy2DAsync(static_cast<char *>(C) + c0 * out_elt, N * out_elt, cj,
+                                  ldN * out_elt, (c1 - c0) * out_elt, rows,
+                                  cudaMemcpyDeviceToHost, c->stream_d2h);
+        if (e != cudaSuccess) {
+            drain();
+            return fail(FG_ERR_CUDA, "chain download: %s", cudaGetErrorString(e));
+        }
+    }
+    CUDA_TRY(cudaStreamSynchronize(c->stream_d2h));
     if ((st = collect_status(c))) return st;
     return ok();
 }

@@ -67,6 +67,11 @@ struct DevCtx {
     int sms = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    // host-pointer chains: uploads and downloads on their own streams, so that the
+    // copies of one column chunk overlap the compute of another
+    static constexpr int kCopyChunks = 4;
+    cudaStream_t stream_h2d = nullptr, stream_d2h = nullptr;
+    cudaEvent_t ev_up[kCopyChunks] = {}, ev_done[kCopyChunks] = {};
     std::mutex mu;
     char *arena = nullptr;
     size_t arena_cap = 0;
