@@ -244,11 +244,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
                 const CUtensorMap *tm_b = &cs.tm_x;
                 const int a_row = a_tail ? ma - cs.a.tail_row0 : ma;
                 const int b_col = n0 + (BN / 2) * (int)rank;
-                int rows_ready = 0;  // streaming: input row tiles known stored
-                for (int kb = 0; kb < num_kb; ++kb) {
-                    if (row_cnt && (kb * G::BK) / 256 >= rows_ready && rows_ready < row_tiles) {
-                        // first k-block of input row tile g: wait until it is stored
-                        const int g = min((kb * G::BK) / 256, row_tiles - 1);
+                // k-blocks in segments: the whole K at once, or, streaming, one input
+                // row tile (256 / BK k-blocks) after its counter is complete; the
+                // inner loop carries no dependency check
+                constexpr int kKbPerRow = 256 / G::BK;
+                static_assert(256 % G::BK == 0, "k-blocks tile the 256-row input tiles");
+                for (int kb0 = 0; kb0 < num_kb;) {
+                    int kb1 = num_kb;
+                    if (row_cnt) {
+                        const int g = min(kb0 / kKbPerRow, row_tiles - 1);
                         if (ld_acquire_gpu(row_cnt + g) < kDoneIncrementsPerTile) {
                             const uint64_t t0 = globaltimer_ns();
                             while (ld_acquire_gpu(row_cnt + g) < kDoneIncrementsPerTile) {
@@ -261,28 +265,31 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
                             }
                         }
                         fence_proxy_async_global();
-                        rows_ready = g + 1;
+                        if (g + 1 < row_tiles) kb1 = min(num_kb, (g + 1) * kKbPerRow);
                     }
-                    if (!mbar_wait(&bars->empty[s], ph ^ 1, status, KERR_WAIT_EMPTY)) {
-                        set_abort(bars);
-                        goto producer_done;
+                    for (int kb = kb0; kb < kb1; ++kb) {
+                        if (!mbar_wait(&bars->empty[s], ph ^ 1, status, KERR_WAIT_EMPTY)) {
+                            set_abort(bars);
+                            goto producer_done;
+                        }
+                        uint8_t *st = smem + s * G::STAGE_BYTES;
+                        const uint32_t full_leader = mapa_shared(smem_u32(&bars->full[s]), 0);
+                        if (leader) mbar_arrive_expect_tx(&bars->full[s], (uint32_t)tx);
+                        const int k0 = kb * G::BK;
+                        if (my_a) tma_load_2d_pair(st, tm_a, full_leader, k0, a_row);
+                        for (int j = 0; j < my_boxes; ++j)
+                            tma_load_2d_pair(st + G::A_BYTES + j * G::BOX_BYTES, tm_b, full_leader,
+                                             b_col + j * G::BOX_N, k0);
+                        if (leader) {
+                            pending |= 1u << s;
+                            pending_ph = (pending_ph & ~(1u << s)) | (ph << s);
+                        }
+                        if (++s == S) {
+                            s = 0;
+                            ph ^= 1;
+                        }
                     }
-                    uint8_t *st = smem + s * G::STAGE_BYTES;
-                    const uint32_t full_leader = mapa_shared(smem_u32(&bars->full[s]), 0);
-                    if (leader) mbar_arrive_expect_tx(&bars->full[s], (uint32_t)tx);
-                    const int k0 = kb * G::BK;
-                    if (my_a) tma_load_2d_pair(st, tm_a, full_leader, k0, a_row);
-                    for (int j = 0; j < my_boxes; ++j)
-                        tma_load_2d_pair(st + G::A_BYTES + j * G::BOX_BYTES, tm_b, full_leader,
-                                         b_col + j * G::BOX_N, k0);
-                    if (leader) {
-                        pending |= 1u << s;
-                        pending_ph = (pending_ph & ~(1u << s)) | (ph << s);
-                    }
-                    if (++s == S) {
-                        s = 0;
-                        ph ^= 1;
-                    }
+                    kb0 = kb1;
                 }
                 trace_put(P, t, rank, TR_PROD_END, globaltimer_ns());
                 if (aborted(bars)) break;
