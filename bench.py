@@ -1,9 +1,20 @@
 """Benchmark of the flashgemm hot path on B200: one JSON line on stdout.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload bf16-chain|int8-chain|f32-gemm|bf16-gemm|int8-gemm|f32-groups|serve]
+                    [--workload all|bf16-chain|int8-chain|f32-gemm|bf16-gemm|int8-gemm|
+                                f32-groups|serve]
 
-A step is one pass of the hot path over one batch: by default the BF16 chain
+By default (--workload all) the line's headline is the BF16 chain below, and
+the same line carries the rest of the metric as sub-objects, each with its
+own roofline, clocks, end-to-end figure and reference CPU baseline:
+"int8_chain" (the INT8 chain of 4 GEMMs), "f32_gemm" (the 1024^3 FP32 SGEMM on
+the plain FMA kernel), "f32_groups" (128 of the grouped FP32 chains, 2 of them
+tall-skinny, as one graph-captured 3xTF32 launch) and "serve" (the serving
+loop at 0.6 x its measured capacity, 4000 Poisson requests, p50/p99 latency),
+plus "peaks_this_run" (cuBLAS BF16 / INT8 / TF32 / FP32 bursts at 8192^3, the
+denominators the peaks file does not hold).
+
+A step is one pass of the hot path over one batch: the BF16 chain
 of three GEMMs C = A3*(A2*(A1*B)) with B 1024 x 4096 (the activations X
 [4096 x 1024] of X*W1*W2*W3, in the reference's orientation) and weights
 4096 x 1024, 1024 x 4096, 1024 x 1024, BF16 inputs, FP32 accumulation, BF16
@@ -354,7 +365,9 @@ def group_host_inputs(specs, indices, seed):
     return out
 
 
-def run_groups(args, world, rank, local_rank):
+def run_groups(args, world, rank, local_rank, g=None):
+    """Grouped FP32 chains. g: the shared GPU context (None: the reference arm).
+    Returns the line (a dict) on rank 0 of our arm, else None."""
     seed = 4321
     n = max(8, args.group_chains)
     nsk = n if args.skinny_only else max(1, GROUP_SKINNY * n // GROUP_CHAINS)
@@ -375,7 +388,7 @@ def run_groups(args, world, rank, local_rank):
             return 0
         host = group_host_inputs(specs, sample, seed)
         tf, descr, times = group_cpu(specs, sample, host, steps=args.steps)
-        line = {"impl": "reference", "metric": metric, "value": tf, "unit": "TFLOP/s",
+        return {"impl": "reference", "metric": metric, "value": tf, "unit": "TFLOP/s",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1e3 * statistics.median(times), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -383,21 +396,8 @@ def run_groups(args, world, rank, local_rank):
                 "cpu_baseline": dict(descr, value=tf, unit="TFLOP/s"),
                 "e2e": {"value": tf, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return 0
 
-    import torch
-    import flashgemm_b200 as fg
-
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=dev)
-    fg.lib()
+    torch, fg, dist, dev = g.torch, g.fg, g.dist, g.dev
     # operands: weights registered once (resident), activations and outputs in HBM;
     # chain j draws from seed + j (+ rank offset), on the device
     chains = []
@@ -420,7 +420,7 @@ def run_groups(args, world, rank, local_rank):
         chains.append((C, B, N, W))
     t_gen = time.perf_counter() - t_gen
     weight_bytes = sum(w.nbytes for c in chains for w in c[3])
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    flush = g.flush
 
     def timed(plan, sampler=None):
         for _ in range(max(args.warmup, 3)):
@@ -549,9 +549,8 @@ def run_groups(args, world, rank, local_rank):
             w.release()
     if dist:
         dist.barrier()
-        dist.destroy_process_group()
     if rank != 0:
-        return 0
+        return None
 
     # ---- accuracy against FP64 on the sample (host)
     err_x3, err_ff = [], []
@@ -608,8 +607,7 @@ def run_groups(args, world, rank, local_rank):
     if world == 1:
         tf, descr, _ = group_cpu(specs, sample, host, budget_s=args.cpu_budget)
         line["cpu_baseline"] = dict(descr, value=tf, unit="TFLOP/s")
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 # ---------------------------------------------------------------- serving stream
@@ -701,7 +699,9 @@ def serve_cpu_inputs(sets, reqs, seed):
     return host
 
 
-def run_serve(args, world, rank, local_rank):
+def run_serve(args, world, rank, local_rank, g=None):
+    """Serving loop at fractions of its measured capacity. g: the shared GPU
+    context (None: the reference arm). Returns the line on rank 0, else None."""
     seed = 777
     sets = serve_sets(seed)
     nreq = args.serve_requests
@@ -720,7 +720,7 @@ def run_serve(args, world, rank, local_rank):
             return 0
         host = serve_cpu_inputs(sets, cpu_sample, seed + 6)
         tf, descr, times = serve_cpu(sets, cpu_sample, host, steps=args.steps)
-        line = {"impl": "reference", "metric": metric, "value": tf, "unit": "TFLOP/s",
+        return {"impl": "reference", "metric": metric, "value": tf, "unit": "TFLOP/s",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1e3 * statistics.median(times), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "bf16/int8/f32 mix",
@@ -728,20 +728,8 @@ def run_serve(args, world, rank, local_rank):
                 "cpu_baseline": dict(descr, value=tf, unit="TFLOP/s"),
                 "e2e": {"value": tf, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return 0
 
-    import torch
-    import flashgemm_b200 as fg
-
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
-    fg.lib()
+    torch, fg, dist, dev = g.torch, g.fg, g.dist, g.dev
     fg.set_semantics("ref")
     fg.set_f32_algo("3xtf32")
     tdt = {"bf16": torch.bfloat16, "int8": torch.int8, "f32": torch.float32}
@@ -882,9 +870,8 @@ def run_serve(args, world, rank, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         lat = [float(x) for x in t.tolist()]
         dist.barrier()
-        dist.destroy_process_group()
     if rank != 0:
-        return 0
+        return None
 
     top = points[-1]
     peaks, peak_src = load_peaks()
@@ -924,83 +911,107 @@ def run_serve(args, world, rank, local_rank):
         host = serve_cpu_inputs(sets, cpu_sample, seed + 6)
         tf, descr, _ = serve_cpu(sets, cpu_sample, host, budget_s=args.cpu_budget)
         line["cpu_baseline"] = dict(descr, value=tf, unit="TFLOP/s")
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=None,
-                    help="timed steps (default 1000; f32-groups 20)")
-    ap.add_argument("--warmup", type=int, default=None,
-                    help="untimed steps (default 20; f32-groups 3)")
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="bf16-chain",
-                    choices=list(WORKLOADS) + ["f32-groups", "serve"])
-    ap.add_argument("--group-chains", type=int, default=512,
-                    help="f32-groups: chains in the group (fewer: a small case for profiling)")
-    ap.add_argument("--skinny-only", action="store_true",
-                    help="f32-groups: only the tall-skinny chains (a small HBM-bound profiling case)")
-    ap.add_argument("--serve-requests", type=int, default=20000,
-                    help="serve: Poisson requests per rate point")
-    ap.add_argument("--serve-rates", type=float, nargs="+", default=[0.3, 0.6, 0.9],
-                    help="serve: offered rates as fractions of the measured capacity")
-    ap.add_argument("--e2e-steps", type=int, default=None,
-                    help="steps of the host-buffer C-ABI measurement (default: min(steps, 200))")
-    ap.add_argument("--cpu-budget", type=float, default=12.0,
-                    help="seconds of reference CPU work for the cpu_baseline leg")
-    args = ap.parse_args()
-    grouped = args.workload == "f32-groups"
-    if args.steps is None:
-        args.steps = 20 if grouped else 1000
-    if args.warmup is None:
-        args.warmup = 3 if grouped else 20
+class GpuCtx:
+    """What every workload of our arm shares: torch, the library, the process
+    group (N > 1), this rank's device and the L2-flush buffer."""
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if grouped:
-        return run_groups(args, world, rank, local_rank)
-    if args.workload == "serve":
-        return run_serve(args, world, rank, local_rank)
-    dt, N, K1, Ms = WORKLOADS[args.workload]
+    def __init__(self, world, rank, local_rank):
+        import torch
+        import flashgemm_b200 as fg
+        self.torch, self.fg = torch, fg
+        self.world, self.rank, self.local_rank = world, rank, local_rank
+        torch.cuda.set_device(local_rank)
+        self.dev = torch.device("cuda", local_rank)
+        self.dist = None
+        if world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=self.dev)
+            self.dist = dist
+        fg.lib()
+        fg.set_semantics("ref")
+        fg.flashgemm_set_thread_num(1)
+        # written between timed steps (outside their events): larger than the 126 MB L2
+        self.flush = torch.empty(256 << 20, dtype=torch.uint8, device=self.dev)
+
+    def max_over_ranks(self, *vals):
+        if not self.dist:
+            return vals
+        t = self.torch.tensor(list(vals), dtype=self.torch.float64, device=self.dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return tuple(float(x) for x in t.tolist())
+
+    def close(self):
+        if self.dist:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def measure_peaks(g, iters=20):
+    """cuBLAS bursts at 8192^3 on this device in this run (torch): BF16, INT8
+    (torch._int_mm), TF32 and plain FP32 (TF32 off) - the denominators of the
+    dtypes the peaks file does not measure."""
+    torch = g.torch
+    n = 8192
+    out = {}
+    a16 = torch.randn(n, n, device=g.dev).to(torch.bfloat16)
+    a8 = torch.randint(-127, 128, (n, n), device=g.dev, dtype=torch.int8)
+    a32 = torch.randn(n, n, device=g.dev)
+    prev = torch.backends.cuda.matmul.allow_tf32
+
+    def burst(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize(g.dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(iters):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(g.dev)
+        return 2.0 * n ** 3 * iters / (e0.elapsed_time(e1) / 1e3) / 1e12
+
+    try:
+        out["bf16_tflops"] = burst(lambda: a16 @ a16)
+        out["int8_tops"] = burst(lambda: torch._int_mm(a8, a8))
+        torch.backends.cuda.matmul.allow_tf32 = True
+        out["tf32_tflops"] = burst(lambda: a32 @ a32)
+        torch.backends.cuda.matmul.allow_tf32 = False
+        out["fp32_tflops"] = burst(lambda: a32 @ a32)
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    del a16, a8, a32
+    torch.cuda.empty_cache()
+    out["shape"] = "8192^3, cuBLAS through torch, 20-launch burst after 3 warm-up launches"
+    return out
+
+
+def pageable(a):
+    """A copy of `a` in ordinary (pageable) host memory, as the reference's
+    callers pass it (posix_memalign / malloc, multigemm/test/test_bf16_3.c:90-102)."""
+    b = np.empty_like(a)
+    b[...] = a
+    return b
+
+
+def run_chain_bench(args, g, workload, peaks_run=None):
+    """One chain workload (or the FP32 SGEMM) on this rank: device-resident steps,
+    the per-GEMM and cuBLAS comparators, end to end through the C ABI from pinned
+    and from pageable host buffers, the roofline of the main kernel and the
+    reference's CPU time. Returns the line on rank 0, else None."""
+    torch, fg, dist, dev = g.torch, g.fg, g.dist, g.dev
+    world, rank = g.world, g.rank
+    dt, N, K1, Ms = WORKLOADS[workload]
     metric = {"f32": "FP32 GEMM TFLOP/s"}.get(dt, "fused GEMM-chain TFLOP/s")
-    config = {"workload": DESCR[args.workload], "dtype": dt, "N": N, "K1": K1, "M": Ms,
+    config = {"workload": DESCR[workload], "dtype": dt, "N": N, "K1": K1, "M": Ms,
               "gflop_per_step_per_gpu": flops_of(N, K1, Ms) / 1e9,
               "semantics": "reference (panel permutation, INT8 tail rows)",
               "l2": "flushed between steps (256 MiB write outside the step events)",
               "parallelism": f"dp{world} (activation columns partitioned, no collective)"}
-
-    if args.impl == "reference":
-        if rank != 0:
-            return 0
-        tf, descr, times = time_cpu(args.workload, steps=args.steps, warmup=args.warmup)
-        line = {"impl": "reference", "metric": metric, "value": tf, "unit": "TFLOP/s",
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": 1e3 * statistics.median(times), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": dt,
-                "data": "synthetic (seeded)", "config": config,
-                "cpu_baseline": dict(descr, value=tf, unit="TFLOP/s"),
-                "e2e": {"value": tf, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return 0
-
-    import torch
-    import flashgemm_b200 as fg
-
-    torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local_rank))
-    dev = torch.device("cuda", local_rank)
-    fg.lib()
-    fg.set_semantics("ref")
-    fg.flashgemm_set_thread_num(1)
 
     # --------------------------------------------------------- device-resident step
     B, As, Ks = make_inputs(dt, N, K1, Ms, seed=1234 + rank)
@@ -1016,7 +1027,7 @@ def main():
     tA = [to_dev(a) for a in As]
     tC = torch.empty((Ms[-1], N), dtype=torch.int32 if dt == "int8" else torch.float32,
                      device=dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    flush = g.flush
 
     if dt == "f32":
         def step():
@@ -1032,25 +1043,25 @@ def main():
     torch.cuda.synchronize(dev)
     fg.sync()
 
-    def timed_steps(sampler=None):
+    def timed(fn, sampler=None, prof=False):
         """Exactly args.steps steps, each bracketed by CUDA events on torch's
-        stream (the library orders its own stream after it and back), L2
-        flushed between steps outside the events. Returns (sum of step ms,
-        wall seconds, our kernel launches, profile of the stage kernel)."""
+        stream (the library runs on that stream), L2 flushed between steps
+        outside the events. Returns (sum of step ms, wall s, our launches,
+        profile of the main kernel class)."""
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         if dist:
             dist.barrier()
         torch.cuda.synchronize(dev)
         l0 = fg.kernel_launches()
-        fg.profile_begin()
-        ctx = sampler if sampler is not None else _Null()
-        with ctx:
+        if prof:
+            fg.profile_begin()
+        with (sampler if sampler is not None else _Null()):
             t_wall = time.perf_counter()
             for i in range(args.steps):
                 flush.fill_(i & 0xFF)
                 starts[i].record()
-                step()
+                fn()
                 stops[i].record()
             torch.cuda.synchronize(dev)
             fg.sync()
@@ -1058,13 +1069,15 @@ def main():
         if dist:
             dist.barrier()
         torch.cuda.synchronize(dev)
-        fg.profile_end()
-        prof = fg.profile_query(kind)
+        kp = None
+        if prof:
+            fg.profile_end()
+            kp = fg.profile_query(kind)
         return (sum(s.elapsed_time(e) for s, e in zip(starts, stops)), t_wall,
-                fg.kernel_launches() - l0, prof)
+                fg.kernel_launches() - l0, kp)
 
-    sampler = ClockSampler(torch.cuda.current_device() if world == 1 else local_rank)
-    total_ms, t_wall, launches, (k_ms, k_n, k_fl) = timed_steps(sampler)
+    sampler = ClockSampler(torch.cuda.current_device())
+    total_ms, t_wall, launches, (k_ms, k_n, k_fl) = timed(step, sampler, prof=True)
 
     # the same steps through the plain per-GEMM path (one launch per GEMM)
     per_gemm = None
@@ -1072,126 +1085,124 @@ def main():
         fg.set_chain_mode("per_gemm")
         for _ in range(max(args.warmup, 3)):
             step()
-        pg_ms, _, pg_launches, _ = timed_steps()
+        pg_ms, _, pg_launches, _ = timed(step)
         fg.set_chain_mode("fused")
         per_gemm = (pg_ms, pg_launches)
 
     # a plain library path beside it: one cuBLAS GEMM per stage (torch), the
     # narrowing between stages as separate kernels, intermediates in HBM (same
     # shapes and dtypes; INT8 with signed weights, cuBLAS having no unsigned x
-    # signed GEMM; no panel permutation)
-    cublas = None
-    if dt != "f32":
-        if dt == "bf16":
-            cA = [a.view(torch.bfloat16) for a in tA]
-            cB = tB.view(torch.bfloat16)
+    # signed GEMM; no panel permutation). FP32: cuBLAS SGEMM with TF32 off.
+    if dt == "bf16":
+        cA = [a.view(torch.bfloat16) for a in tA]
+        cB = tB.view(torch.bfloat16)
 
-            def plain():
-                x = cB
-                for a in cA:
-                    x = a @ x  # FP32 accumulation, BF16 result (RNE)
-                return x.float()
-        else:
-            cA = list(tA)
-            cB = tB
-
-            def plain():
-                x = cB
-                for i, a in enumerate(cA):
-                    y = torch._int_mm(a, x)
-                    x = y if i == len(cA) - 1 else y.clamp_(-128, 127).to(torch.int8)
-                return x
+        def plain():
+            x = cB
+            for a in cA:
+                x = a @ x  # FP32 accumulation, BF16 result (RNE)
+            return x.float()
+    elif dt == "int8":
+        def plain():
+            x = tB
+            for i, a in enumerate(tA):
+                y = torch._int_mm(a, x)
+                x = y if i == len(tA) - 1 else y.clamp_(-128, 127).to(torch.int8)
+            return x
+    else:
+        def plain():
+            return torch.matmul(tA[0], tB, out=tC)
+    prev_tf32 = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
         for _ in range(max(args.warmup, 3)):
             plain()
-        torch.cuda.synchronize(dev)
-        cs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        ce = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        for i in range(args.steps):
-            flush.fill_(i & 0xFF)
-            cs[i].record()
-            plain()
-            ce[i].record()
-        torch.cuda.synchronize(dev)
-        cublas = sum(a.elapsed_time(b) for a, b in zip(cs, ce))
+        cublas, _, _, _ = timed(plain)
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev_tf32
 
-    # max over ranks
-    if dist:
-        t = torch.tensor([total_ms, per_gemm[0] if per_gemm else 0.0], dtype=torch.float64,
-                         device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t[0].item())
-        if per_gemm:
-            per_gemm = (float(t[1].item()), per_gemm[1])
+    total_ms, = g.max_over_ranks(total_ms)
+    if per_gemm:
+        per_gemm = (g.max_over_ranks(per_gemm[0])[0], per_gemm[1])
     step_flops = flops_of(N, K1, Ms)
     value = world * step_flops * args.steps / (total_ms / 1e3) / 1e12
 
     # --------------------------------------------------------- end to end through the C ABI
     e2e_steps = args.e2e_steps or min(args.steps, 200)
-    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
-    hB = pin(B)
-    hA = [pin(a) for a in As]
-    hC = pin(np.zeros((Ms[-1], N), np.int32 if dt == "int8" else np.float32))
-    trip = []
-    for a, m, k in zip(hA, Ms, Ks):
-        trip += [a, m, k]
-    if dt == "f32":
-        def e2e_step():
-            fg.LibShalom_sgemm_mp(0, 0, hC, hA[0], hB, Ms[0], N, K1, check=True)
-    else:
-        fn = {"bf16": fg.flashgemm_multi_bf16bf16f32,
-              "int8": fg.flashgemm_multi_int8uint8int32}[dt]
 
-        def e2e_step():
-            fn(hC, hB, N, len(Ms), *trip, check=True)
-    for _ in range(3):
-        e2e_step()
-    if dist:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        e2e_step()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * step_flops * e2e_steps / e2e_s / 1e12
+    def e2e_run(hB, hA, hC):
+        trip = []
+        for a, m, k in zip(hA, Ms, Ks):
+            trip += [a, m, k]
+        if dt == "f32":
+            def one():
+                fg.LibShalom_sgemm_mp(0, 0, hC, hA[0], hB, Ms[0], N, K1, check=True)
+        else:
+            fn = {"bf16": fg.flashgemm_multi_bf16bf16f32,
+                  "int8": fg.flashgemm_multi_int8uint8int32}[dt]
+
+            def one():
+                fn(hC, hB, N, len(Ms), *trip, check=True)
+        for _ in range(3):
+            one()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            one()
+        sec, = g.max_over_ranks(time.perf_counter() - t0)
+        return world * step_flops * e2e_steps / sec / 1e12
+
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+    out_np = np.int32 if dt == "int8" else np.float32
+    hB, hA, hC = pin(B), [pin(a) for a in As], pin(np.zeros((Ms[-1], N), out_np))
+    e2e_value = e2e_run(hB, hA, hC)
+    pB, pA, pC = pageable(B), [pageable(a) for a in As], np.zeros((Ms[-1], N), out_np)
+    e2e_pageable = e2e_run(pB, pA, pC)
     h2d = hB.nbytes + sum(a.nbytes for a in hA)
     d2h = hC.nbytes
+    del hB, hA, hC, pB, pA, pC
 
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
     if rank != 0:
-        return 0
-
+        return None
     peaks, peak_src = load_peaks()
+    peaks_run = peaks_run or {}
     achieved = k_fl / (k_ms / 1e3) / 1e12 if k_ms > 0 else None
     if dt == "bf16":
-        peak, peak_name = peaks.get("bf16_tflops"), "bf16_tflops (cuBLAS BF16 burst, measured)"
+        peak, peak_name = peaks.get("bf16_tflops"), "bf16_tflops (cuBLAS BF16 burst)"
+        peak_src_s = peak_src
     elif dt == "int8":
-        # no INT8 measurement in the peaks file: the B200's dense INT8 rate is twice
-        # its BF16 rate per clock, so twice the measured BF16 figure stands in
-        peak = 2 * peaks.get("bf16_tflops")
-        peak_name = "2 x bf16_tflops (INT8 = 2x BF16 per clock; measured BF16)"
+        if peaks_run.get("int8_tops"):
+            peak = peaks_run["int8_tops"]
+            peak_name = "cuBLAS INT8 burst at 8192^3 (torch._int_mm), measured in this run"
+            peak_src_s = "measured"
+        else:
+            peak = 2 * peaks.get("bf16_tflops")
+            peak_name = "2 x bf16_tflops (INT8 = 2x BF16 per clock)"
+            peak_src_s = peak_src
     else:
         sm_mhz = peaks.get("sm_max_mhz", 1965.0)
         peak = 148 * 256 * sm_mhz * 1e6 / 1e12
         peak_name = "148 SMs x 128 FFMA/clk x 2 x sm_max_mhz (datasheet-style FFMA peak)"
+        peak_src_s = "datasheet arithmetic"
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            traffic = json.load(f).get(args.workload)
+            traffic = json.load(f).get(workload)
     except (OSError, ValueError):
         traffic = None
-    roofline = {"bound": "tensor" if dt != "f32" else "tensor", "achieved": achieved,
+    roofline = {"bound": "tensor" if dt != "f32" else "ffma", "achieved": achieved,
                 "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved and peak else None,
                 "traffic": traffic.get("bytes_per_launch") if traffic else None,
                 "kernel": ("fg::tc_chain_kernel (whole chain, one launch)" if dt != "f32"
                            else "fg::ffma_sgemm_kernel"),
                 "launches_timed": k_n, "avg_launch_us": 1e3 * k_ms / k_n if k_n else None,
-                "peak_source": f"{peak_name}; {peak_src}"}
+                "peak_source": f"{peak_name}; {peak_src_s}"}
+    if dt == "int8":
+        roofline["frac_of_2x_bf16"] = achieved / (2 * peaks.get("bf16_tflops")) if achieved else None
+    if dt == "f32" and peaks_run.get("fp32_tflops"):
+        roofline["frac_of_cublas_fp32_burst"] = achieved / peaks_run["fp32_tflops"] if achieved else None
 
     line = {"metric": metric, "value": value, "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -1200,7 +1211,9 @@ def main():
             "clocks": sampler.summary(), "gpu_launches": launches,
             "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps,
-                    "api": "flashgemm_multi_*/LibShalom_sgemm_mp, pinned host buffers"},
+                    "api": "flashgemm_multi_*/LibShalom_sgemm_mp, pinned host buffers",
+                    "pageable_value": e2e_pageable,
+                    "pageable_api": "the same calls on ordinary (pageable) host buffers"},
             "roofline": roofline, "wall_s_timed_region": t_wall}
     if per_gemm:
         pg_value = world * step_flops * args.steps / (per_gemm[0] / 1e3) / 1e12
@@ -1209,17 +1222,140 @@ def main():
                             "launches": per_gemm[1],
                             "path": "one tensor-core launch per GEMM (FG_CHAIN_PER_GEMM)"}
         line["fused_vs_per_gemm"] = value / pg_value
-    if cublas:
-        cb_value = world * step_flops * args.steps / (cublas / 1e3) / 1e12
+    cb_value = world * step_flops * args.steps / (cublas / 1e3) / 1e12
+    if dt == "f32":
+        line["cublas_sgemm"] = {"value": cb_value, "unit": "TFLOP/s",
+                                "ms_per_step": cublas / args.steps,
+                                "path": "torch.matmul FP32 (cuBLAS SGEMM, TF32 off), same operands"}
+        line["ffma_vs_cublas_sgemm"] = value / cb_value
+    else:
         line["cublas_per_gemm"] = {
             "value": cb_value, "unit": "TFLOP/s", "ms_per_step": cublas / args.steps,
             "path": "torch.matmul / torch._int_mm (cuBLAS) per GEMM, narrowing as separate "
                     "kernels, intermediates in HBM; INT8 with signed weights, no panel permutation"}
         line["fused_vs_cublas_per_gemm"] = value / cb_value
     if world == 1:
-        tf, descr, _ = time_cpu(args.workload, budget_s=args.cpu_budget)
+        tf, descr, _ = time_cpu(workload, budget_s=args.cpu_budget)
         line["cpu_baseline"] = dict(descr, value=tf, unit="TFLOP/s")
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def reference_line(args, workload):
+    """--impl reference for a chain / SGEMM workload: the reference's own CPU
+    implementation on all host threads, on a bounded column sample."""
+    dt, N, K1, Ms = WORKLOADS[workload]
+    metric = {"f32": "FP32 GEMM TFLOP/s"}.get(dt, "fused GEMM-chain TFLOP/s")
+    config = {"workload": DESCR[workload], "dtype": dt, "N": N, "K1": K1, "M": Ms,
+              "gflop_per_step_per_gpu": flops_of(N, K1, Ms) / 1e9,
+              "semantics": "reference (panel permutation, INT8 tail rows)",
+              "l2": "flushed between steps (256 MiB write outside the step events)",
+              "parallelism": f"dp{args.gpus} (activation columns partitioned, no collective)"}
+    tf, descr, times = time_cpu(workload, steps=args.steps, warmup=args.warmup)
+    return {"impl": "reference", "metric": metric, "value": tf, "unit": "TFLOP/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * statistics.median(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dt,
+            "data": "synthetic (seeded)", "config": config,
+            "cpu_baseline": dict(descr, value=tf, unit="TFLOP/s"),
+            "e2e": {"value": tf, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+# keys of a sub-object: the workload's own figures, without the top-level
+# contract fields it shares with the headline line
+_SUB_DROP = ("n_gpus", "warmup", "higher_is_better", "scaling", "vs_baseline", "data")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 200; f32-groups 20)")
+    ap.add_argument("--warmup", type=int, default=None,
+                    help="untimed steps (default 10; f32-groups 3)")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="all",
+                    choices=["all"] + list(WORKLOADS) + ["f32-groups", "serve"],
+                    help="all (default): the BF16 chain as the headline line, with the INT8 "
+                         "chain, the FP32 SGEMM, a grouped FP32 subset and a serving point as "
+                         "sub-objects of the same line")
+    ap.add_argument("--group-chains", type=int, default=None,
+                    help="f32-groups: chains in the group (default 512; 128 within 'all')")
+    ap.add_argument("--skinny-only", action="store_true",
+                    help="f32-groups: only the tall-skinny chains (a small HBM-bound profiling case)")
+    ap.add_argument("--serve-requests", type=int, default=None,
+                    help="serve: Poisson requests per rate point (default 20000; 4000 within 'all')")
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=None,
+                    help="serve: offered rates as fractions of the measured capacity "
+                         "(default 0.3 0.6 0.9; 0.6 within 'all')")
+    ap.add_argument("--e2e-steps", type=int, default=None,
+                    help="steps of the host-buffer C-ABI measurement (default: min(steps, 200))")
+    ap.add_argument("--cpu-budget", type=float, default=None,
+                    help="seconds of reference CPU work for each cpu_baseline leg "
+                         "(default 12; 6 within 'all')")
+    args = ap.parse_args()
+    combined = args.workload == "all"
+    grouped = args.workload == "f32-groups"
+    if args.steps is None:
+        args.steps = 20 if grouped else 200
+    if args.warmup is None:
+        args.warmup = 3 if grouped else 10
+    if args.group_chains is None:
+        args.group_chains = 128 if combined else GROUP_CHAINS
+    if args.serve_requests is None:
+        args.serve_requests = 4000 if combined else 20000
+    if args.serve_rates is None:
+        args.serve_rates = [0.6] if combined else [0.3, 0.6, 0.9]
+    if args.cpu_budget is None:
+        args.cpu_budget = 6.0 if combined else 12.0
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        # rank 0 alone times the reference's CPU implementation; the others exit
+        if rank != 0:
+            return 0
+        if grouped:
+            line = run_groups(args, world, rank, local_rank)
+        elif args.workload == "serve":
+            line = run_serve(args, world, rank, local_rank)
+        else:
+            line = reference_line(args, "bf16-chain" if combined else args.workload)
+        print(json.dumps(line), flush=True)
+        return 0
+
+    g = GpuCtx(world, rank, local_rank)
+    if grouped:
+        line = run_groups(args, world, rank, local_rank, g)
+    elif args.workload == "serve":
+        line = run_serve(args, world, rank, local_rank, g)
+    elif not combined:
+        line = run_chain_bench(args, g, args.workload)
+    else:
+        peaks_run = measure_peaks(g)
+        line = run_chain_bench(args, g, "bf16-chain", peaks_run)
+        subs = {}
+        subs["int8_chain"] = run_chain_bench(args, g, "int8-chain", peaks_run)
+        subs["f32_gemm"] = run_chain_bench(args, g, "f32-gemm", peaks_run)
+        gargs = argparse.Namespace(**vars(args))
+        gargs.steps, gargs.warmup = min(args.steps, 20), 3
+        subs["f32_groups"] = run_groups(gargs, world, rank, local_rank, g)
+        subs["serve"] = run_serve(args, world, rank, local_rank, g)
+        if rank == 0:
+            for k, v in subs.items():
+                line[k] = {kk: vv for kk, vv in v.items() if kk not in _SUB_DROP}
+            line["gpu_launches_all_workloads"] = line["gpu_launches"] + sum(
+                v.get("gpu_launches") or 0 for v in subs.values())
+            line["peaks_this_run"] = peaks_run
+            grp = subs["f32_groups"]
+            if grp.get("roofline") and peaks_run.get("tf32_tflops"):
+                r = grp["roofline"]
+                r["frac_of_measured_tf32_div3"] = r["achieved"] / (peaks_run["tf32_tflops"] / 3.0)
+    g.close()
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
     return 0
 
 

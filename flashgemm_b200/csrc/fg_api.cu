@@ -143,6 +143,7 @@ int get_ctx(DevCtx **out)
         c->dev = dev;
         c->sms = prop.multiProcessorCount;
         CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->work = c->stream;
         CUDA_TRY(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
         CUDA_TRY(cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming));
         CUDA_TRY(cudaStreamCreateWithFlags(&c->stream_h2d, cudaStreamNonBlocking));
@@ -165,7 +166,7 @@ int arena_reserve(DevCtx *c, size_t bytes)
 {
     c->arena_off = 0;
     if (bytes <= c->arena_cap) return FG_OK;
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->work));
     if (c->arena) cudaFree(c->arena);
     c->arena = nullptr;
     c->arena_cap = 0;
@@ -183,7 +184,7 @@ int arena_reserve(DevCtx *c, size_t bytes)
 int tab_reserve(DevCtx *c, size_t bytes)
 {
     if (bytes <= c->tab_cap) return FG_OK;
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->work));
     if (c->tab) cudaFree(c->tab);
     c->tab = nullptr;
     c->tab_cap = 0;
@@ -202,6 +203,44 @@ void *arena_take(DevCtx *c, size_t bytes)
     size_t off = (c->arena_off + 255) & ~(size_t)255;
     c->arena_off = off + bytes;
     return c->arena + off;
+}
+
+int enter_stream(DevCtx *c, cudaStream_t s)
+{
+    if (s == c->work) return FG_OK;
+    CUDA_TRY(cudaEventRecord(c->ev_in, c->work));
+    CUDA_TRY(cudaStreamWaitEvent(s, c->ev_in, 0));
+    c->work = s;
+    return FG_OK;
+}
+
+// Counters are carved in 64-int steps from a block of 1 Mi ints (grown when a
+// launch needs more); a used-up block is zeroed by one memset on the work
+// stream, which every earlier launch precedes, so no launch sees another's counts.
+int take_counters(DevCtx *c, size_t n, int **out)
+{
+    const size_t need = (n + 63) & ~(size_t)63;
+    if (need > c->ctr_cap) {
+        CUDA_TRY(cudaStreamSynchronize(c->work));
+        if (c->ctr) cudaFree(c->ctr);
+        c->ctr = nullptr;
+        c->ctr_cap = 0;
+        const size_t cap = need > (1u << 20) ? need : (1u << 20);
+        cudaError_t e = cudaMalloc(&c->ctr, cap * sizeof(int));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(FG_ERR_NOMEM, "chain counters: %s", cudaGetErrorString(e));
+        }
+        CUDA_TRY(cudaMemsetAsync(c->ctr, 0, cap * sizeof(int), c->work));
+        c->ctr_cap = cap;
+        c->ctr_off = 0;
+    } else if (c->ctr_off + need > c->ctr_cap) {
+        CUDA_TRY(cudaMemsetAsync(c->ctr, 0, c->ctr_cap * sizeof(int), c->work));
+        c->ctr_off = 0;
+    }
+    *out = c->ctr + c->ctr_off;
+    c->ctr_off += need;
+    return FG_OK;
 }
 
 
@@ -294,8 +333,8 @@ int launch_stages(DevCtx *c, int kind, std::vector<StageArgs> &stages, long N)
         std::vector<long> rows(n);
         for (int i = 0; i < n; ++i) rows[i] = stages[i].M;
         const size_t done_ints = chain_counter_ints(n, rows.data(), N);
-        int *done = (int *)arena_take(c, done_ints * sizeof(int));
-        CUDA_TRY(cudaMemsetAsync(done, 0, done_ints * sizeof(int), c->stream));
+        int *done = nullptr;
+        if (int e = take_counters(c, done_ints, &done)) return e;
         double fl = 0.0;
         for (auto &st : stages) fl += gemm_flops(st.M, st.N, st.K);
         // FG_TRACE_DIR=<dir>: write a per-tile timeline of every fused launch there
@@ -308,18 +347,18 @@ int launch_stages(DevCtx *c, int kind, std::vector<StageArgs> &stages, long N)
             for (auto &sa : stages) items += (size_t)((sa.M + 255) / 256) * tiles_n;
             trace_words = items * 2 * chain_trace_fields();
             trace = (unsigned long long *)arena_take(c, trace_words * 8);
-            CUDA_TRY(cudaMemsetAsync(trace, 0, trace_words * 8, c->stream));
+            CUDA_TRY(cudaMemsetAsync(trace, 0, trace_words * 8, c->work));
         }
         cudaError_t le = cudaSuccess;
         int st = run_kernel(c, kind, fl, "fused chain", [&] {
-            le = launch_tc_chain(stages.data(), n, done, c->status, trace, c->sms, c->stream);
+            le = launch_tc_chain(stages.data(), n, done, c->status, trace, c->sms, c->work);
             return le;
         });
         if (st == FG_OK && trace) {
             std::vector<unsigned long long> h(trace_words);
             CUDA_TRY(cudaMemcpyAsync(h.data(), trace, trace_words * 8, cudaMemcpyDeviceToHost,
-                                     c->stream));
-            CUDA_TRY(cudaStreamSynchronize(c->stream));
+                                     c->work));
+            CUDA_TRY(cudaStreamSynchronize(c->work));
             static int seq = 0;
             char path[1024];
             snprintf(path, sizeof path, "%s/chain_trace_%d.csv", trace_dir, seq++);
@@ -350,7 +389,7 @@ int launch_stages(DevCtx *c, int kind, std::vector<StageArgs> &stages, long N)
     for (auto &s : stages) {
         int st = run_kernel(c, kind, gemm_flops(s.M, s.N, s.K),
                             kind == FG_PK_TC_BF16 ? "bf16 stage" : "int8 stage",
-                            [&] { return launch_tc_stage(s, c->sms, c->stream); });
+                            [&] { return launch_tc_stage(s, c->sms, c->work); });
         if (st) return st;
     }
     return FG_OK;
@@ -358,7 +397,7 @@ int launch_stages(DevCtx *c, int kind, std::vector<StageArgs> &stages, long N)
 
 
 // Builds the stage list of a BF16 or INT8 chain (between-stage buffers from the
-// arena, weight preparations launched on c->stream) without launching the stages.
+// arena, weight preparations launched on c->work) without launching the stages.
 int build_tc_stages(DevCtx *c, int dtype, int sem, void *C, long ldc, Mat b, long N, int n,
                     const Mat *a, const long *M, const long *K, const PreparedW *pw,
                     std::vector<StageArgs> &out, Carver *cv)
@@ -387,9 +426,9 @@ int build_tc_stages(DevCtx *c, int dtype, int sem, void *C, long ldc, Mat b, lon
             if ((ldw % 8) || ((uintptr_t)w % 16)) {
                 const long ldk = round_up(K[i], 8);
                 void *wp = take((size_t)M[i] * ldk * 2);
-                CUDA_TRY(cudaMemsetAsync(wp, 0, (size_t)M[i] * ldk * 2, c->stream));
+                CUDA_TRY(cudaMemsetAsync(wp, 0, (size_t)M[i] * ldk * 2, c->work));
                 CUDA_TRY(cudaMemcpy2DAsync(wp, ldk * 2, w, ldw * 2, K[i] * 2, M[i],
-                                           cudaMemcpyDeviceToDevice, c->stream));
+                                           cudaMemcpyDeviceToDevice, c->work));
                 w = wp;
                 ldw = ldk;
             }
@@ -443,7 +482,7 @@ int build_tc_stages(DevCtx *c, int dtype, int sem, void *C, long ldc, Mat b, lon
                 uint8_t *wp = (uint8_t *)take((size_t)Mi * ldw);
                 int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 weight copy", [&] {
                     return launch_prep_int8_weights((const int8_t *)a[i].p, a[i].ld, wp, ldw, Mi,
-                                                    Ki, 0, 0, c->stream);
+                                                    Ki, 0, 0, c->work);
                 });
                 if (st) return st;
                 wmain = wp;
@@ -461,7 +500,7 @@ int build_tc_stages(DevCtx *c, int dtype, int sem, void *C, long ldc, Mat b, lon
                 uint8_t *wt = (uint8_t *)take((size_t)(Mi - row0) * ldw);
                 if (jobs.n == 8) {  // flush a full batch
                     int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 tail-row prep",
-                                        [&] { return launch_prep_int8_jobs(jobs, c->stream); });
+                                        [&] { return launch_prep_int8_jobs(jobs, c->work); });
                     if (st) return st;
                     jobs.n = 0;
                 }
@@ -489,7 +528,7 @@ int build_tc_stages(DevCtx *c, int dtype, int sem, void *C, long ldc, Mat b, lon
         }
         if (jobs.n) {  // all tail blocks of the chain in one launch
             int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 tail-row prep",
-                                [&] { return launch_prep_int8_jobs(jobs, c->stream); });
+                                [&] { return launch_prep_int8_jobs(jobs, c->work); });
             if (st) return st;
         }
         out = std::move(stages);
@@ -498,7 +537,7 @@ int build_tc_stages(DevCtx *c, int dtype, int sem, void *C, long ldc, Mat b, lon
     return fail(FG_ERR_INVALID, "not a tensor-core chain dtype");
 }
 
-// Runs the chain on c->stream. Device operands: B (K[0] x N, ld b.ld),
+// Runs the chain on c->work. Device operands: B (K[0] x N, ld b.ld),
 // A[i] (M[i] x K[i], ld a[i].ld, 16-byte-aligned rows where the tensor path
 // needs them), C (M[n-1] x N, ld ldc). Scratch must already be reserved.
 int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b, long N, int n,
@@ -527,7 +566,7 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             f.ldc = last ? ldc : ldN;
             f.kblock = 0;  // the multigemm FP32 chain does not split K (kernel_f32.h:3)
             int st = run_kernel(c, FG_PK_FFMA, gemm_flops(M[i], N, K[i]), "ffma stage",
-                                [&] { return launch_ffma_sgemm(f, c->sms, c->stream); });
+                                [&] { return launch_ffma_sgemm(f, c->sms, c->work); });
             if (st) return st;
             x = f.C;
             ldx = f.ldc;
@@ -558,14 +597,14 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             wl[i] = l;
             int st = run_kernel(c, FG_PK_AUX, 0.0, "tf32 split (weights)", [&] {
                 return launch_split_tf32((const float *)a[i].p, a[i].ld, h, l, ldk, M[i], K[i],
-                                         c->stream);
+                                         c->work);
             });
             if (st) return st;
         }
         float *xh = (float *)arena_take(c, (size_t)K[0] * ldN * 4);
         float *xl = (float *)arena_take(c, (size_t)K[0] * ldN * 4);
         int st = run_kernel(c, FG_PK_AUX, 0.0, "tf32 split (activations)", [&] {
-            return launch_split_tf32((const float *)b.p, b.ld, xh, xl, ldN, K[0], N, c->stream);
+            return launch_split_tf32((const float *)b.p, b.ld, xh, xl, ldN, K[0], N, c->work);
         });
         if (st) return st;
         float *ph[2] = {nullptr, nullptr}, *pl[2] = {nullptr, nullptr};
@@ -588,7 +627,7 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             s.tail_lo = s.tail_hi = 0;
             s.kchunk = tf32_chunk_blocks(K[i]);
             st = run_kernel(c, FG_PK_TC_TF32X3, gemm_flops(M[i], N, K[i]), "tf32x3 stage",
-                            [&] { return launch_tc_stage(s, c->sms, c->stream); });
+                            [&] { return launch_tc_stage(s, c->sms, c->work); });
             if (st) return st;
             xh = ph[i & 1];
             xl = pl[i & 1];
@@ -604,16 +643,16 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
     }
 }
 
-// Read and clear the device status word (the stream must be idle).
+// Read and clear the device status word (waits for the work stream).
 int collect_status(DevCtx *c)
 {
     CUDA_TRY(cudaMemcpyAsync(c->status_host, c->status, sizeof(int), cudaMemcpyDeviceToHost,
-                             c->stream));
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
+                             c->work));
+    CUDA_TRY(cudaStreamSynchronize(c->work));
     const int code = *c->status_host;
     if (code) {
-        CUDA_TRY(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
-        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        CUDA_TRY(cudaMemsetAsync(c->status, 0, sizeof(int), c->work));
+        CUDA_TRY(cudaStreamSynchronize(c->work));
         return fail(FG_ERR_TIMEOUT, "a kernel's pipeline wait ran out (code 0x%x)", code);
     }
     return FG_OK;
@@ -658,7 +697,11 @@ int host_chain(int dtype, void *C, const void *B, long N, int n, const void *con
         need += carve_size((size_t)M[i] * lda[i] * elt);
     }
     need += chain_scratch(dtype, algo, N, n, M, K) + 4096;
+    if ((st = enter_stream(c, c->stream))) return st;
     if ((st = arena_reserve(c, need))) return st;
+    // the uploads overwrite the arena: after every earlier call's kernels
+    CUDA_TRY(cudaEventRecord(c->ev_in, c->stream));
+    CUDA_TRY(cudaStreamWaitEvent(c->stream_h2d, c->ev_in, 0));
 
     void *bd = arena_take(c, (size_t)K[0] * ldN * elt);
     std::vector<Mat> ad(n);
@@ -758,7 +801,7 @@ int run_sgemm(DevCtx *c, int algo, float *C, long ldc, const float *A, long lda,
         f.A = A; f.lda = lda; f.B = B; f.ldb = ldb; f.C = C; f.ldc = ldc;
         f.kblock = kblock;
         return run_kernel(c, FG_PK_FFMA, gemm_flops(M, N, K), "ffma sgemm",
-                          [&] { return launch_ffma_sgemm(f, c->sms, c->stream); });
+                          [&] { return launch_ffma_sgemm(f, c->sms, c->work); });
     }
     Mat a{A, lda};
     return run_chain(c, FG_DT_F32, FG_SEM_MATH, FG_F32_3XTF32, C, ldc, Mat{B, ldb}, N, 1, &a, &M, &K);
@@ -782,6 +825,7 @@ int host_sgemm(float *C, const float *A, const float *B, long M, long N, long K)
         long Ms[1] = {M}, Ks[1] = {K};
         need += chain_scratch(FG_DT_F32, algo, N, 1, Ms, Ks);
     }
+    if ((st = enter_stream(c, c->stream))) return st;
     if ((st = arena_reserve(c, need))) return st;
     float *ad = (float *)arena_take(c, (size_t)M * ldk * 4);
     float *bd = (float *)arena_take(c, (size_t)(K > 0 ? K : 1) * ldn * 4);
@@ -851,6 +895,7 @@ int register_weights(int dtype, const void *A, long M, long K, int where, fg_wei
     if ((st = get_ctx(&c))) return st;
     std::lock_guard<std::mutex> lk(c->mu);
     const int elt = elt_of(dtype);
+    if ((st = enter_stream(c, c->stream))) return st;
     fg_weights_s *w = new fg_weights_s;
     w->dtype = dtype;
     w->dev = c->dev;
@@ -959,6 +1004,7 @@ using namespace fg::host;
 namespace fg {
 int api_fail(int status, const char *msg) { return host::fail(status, "%s", msg); }
 int api_ok() { return host::ok(); }
+int noalloc_take_status(int dev, int *code);  // fg_noalloc.cu
 }  // namespace fg
 
 // ==================================================================== C ABI
@@ -1089,20 +1135,20 @@ FG_EXPORT int fg_chain_dev(int dtype, void *C, const void *B, long N, int num_ge
     const bool pad_b = tensor && ((N * elt) % 16 != 0);
     size_t need = chain_scratch(dtype, algo, N, num_gemm, M, K) + 4096;
     if (pad_b) need += carve_size((size_t)K[0] * ldN * elt);
+    // the kernels run on the caller's stream itself (after all earlier library work)
+    if ((st = enter_stream(c, user_stream(stream)))) return st;
     if ((st = arena_reserve(c, need))) return st;
-    if ((st = fence_in(c, stream))) return st;
     Mat b{B, N};
     if (pad_b) {
         void *p = arena_take(c, (size_t)K[0] * ldN * elt);
         CUDA_TRY(cudaMemcpy2DAsync(p, ldN * elt, B, N * elt, N * elt, K[0], cudaMemcpyDeviceToDevice,
-                                   c->stream));
+                                   c->work));
         b = Mat{p, ldN};
     }
     std::vector<Mat> a(num_gemm);
     for (int i = 0; i < num_gemm; ++i) a[i] = Mat{A[i], K[i]};
     if ((st = run_chain(c, dtype, semantics(), algo, C, N, b, N, num_gemm, a.data(), M, K)))
         return st;
-    if ((st = fence_out(c, stream))) return st;
     return ok();
 }
 
@@ -1124,10 +1170,9 @@ FG_EXPORT int fg_sgemm_dev(float *C, const float *A, const float *B, long M, lon
         long Ms[1] = {M}, Ks[1] = {K};
         need += chain_scratch(FG_DT_F32, algo, N, 1, Ms, Ks);
     }
+    if ((st = enter_stream(c, user_stream(stream)))) return st;
     if ((st = arena_reserve(c, need))) return st;
-    if ((st = fence_in(c, stream))) return st;
     if ((st = run_sgemm(c, algo, C, N, A, K, B, N, M, N, K, 2048))) return st;
-    if ((st = fence_out(c, stream))) return st;
     return ok();
 }
 
@@ -1137,8 +1182,15 @@ FG_EXPORT int fg_sync(void)
     int st;
     if ((st = get_ctx(&c))) return st;
     std::lock_guard<std::mutex> lk(c->mu);
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->work));
     if ((st = collect_status(c))) return st;
+    // the allocation-free entry point's own status word (calls made with status == NULL)
+    int code = 0;
+    const int e = noalloc_take_status(c->dev, &code);
+    if (e) return fail(FG_ERR_CUDA, "no-alloc status word: %s", cudaGetErrorString((cudaError_t)e));
+    if (code)
+        return fail(FG_ERR_TIMEOUT, "fg_chain_bf16_noalloc: a kernel's pipeline wait ran out "
+                                    "(code 0x%x)", code);
     return ok();
 }
 
@@ -1148,7 +1200,7 @@ FG_EXPORT int fg_profile_begin(void)
     int st;
     if ((st = get_ctx(&c))) return st;
     std::lock_guard<std::mutex> lk(c->mu);
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->work));
     for (auto &r : c->prof) c->prof_pool.push_back(r);
     c->prof.clear();
     g_prof_on.store(1);
@@ -1168,7 +1220,7 @@ FG_EXPORT int fg_profile_query(int kind, double *total_ms, unsigned long long *l
     int st;
     if ((st = get_ctx(&c))) return st;
     std::lock_guard<std::mutex> lk(c->mu);
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->work));
     double ms = 0.0, fl = 0.0;
     unsigned long long n = 0;
     for (auto &r : c->prof) {
@@ -1241,18 +1293,17 @@ FG_EXPORT int fg_chain_registered(int dtype, void *C, const void *B, long N, int
     const bool pad_b = tensor && ((N * elt) % 16 != 0);
     size_t need = chain_scratch(dtype, algo, N, num_gemm, M.data(), K.data()) + 4096;
     if (pad_b) need += carve_size((size_t)K[0] * ldN * elt);
+    if ((st = enter_stream(c, user_stream(stream)))) return st;
     if ((st = arena_reserve(c, need))) return st;
-    if ((st = fence_in(c, stream))) return st;
     Mat b{B, N};
     if (pad_b) {
         void *p = arena_take(c, (size_t)K[0] * ldN * elt);
         CUDA_TRY(cudaMemcpy2DAsync(p, ldN * elt, B, N * elt, N * elt, K[0], cudaMemcpyDeviceToDevice,
-                                   c->stream));
+                                   c->work));
         b = Mat{p, ldN};
     }
     if ((st = run_chain(c, dtype, semantics(), algo, C, N, b, N, num_gemm, a.data(), M.data(),
                         K.data(), pw.data())))
         return st;
-    if ((st = fence_out(c, stream))) return st;
     return ok();
 }

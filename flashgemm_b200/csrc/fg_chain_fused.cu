@@ -31,6 +31,8 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <iterator>
+#include <memory>
 #include <mutex>
 #include <vector>
 
@@ -557,6 +559,18 @@ void set_counters(std::vector<ChainStage> &st, unsigned stream)
 // else none. (Measured on B200: the BF16 chain 4096x1024 -> 4096 -> 1024 ->
 // 1024, estimate 0.978 of block-wise, ran 4 % faster streamed; the INT8 chain
 // 8192x2048 -> 4096 -> 2048 -> 4096 -> 1024, estimate 1.008, 15 % slower.)
+// FG_CHAIN_FEED=0: no feeder workers (see Feeders) in a single chain's schedule;
+// otherwise the host tries them at every streamed boundary and keeps them when
+// the estimate is at least 1 % shorter.
+bool feed_mode()
+{
+    static const bool on = [] {
+        const char *v = getenv("FG_CHAIN_FEED");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
 constexpr unsigned kStreamAuto = ~0u;
 unsigned stream_mode()
 {
@@ -571,16 +585,62 @@ unsigned stream_mode()
 
 }  // namespace
 
+// Everything a chain's launch parameters depend on besides the counters and the
+// trace buffer: the stages' operands, shapes and epilogues, the grid, the mode.
+static std::vector<long> params_key(const StageArgs *st, int n, int device, int num_sms)
+{
+    std::vector<long> k = {device, num_sms, n, (long)stream_mode()};
+    for (int i = 0; i < n; ++i) {
+        const StageArgs &a = st[i];
+        const long v[] = {a.op, a.M, a.N, a.K, (long)a.w, (long)a.w_lo, a.ld_w, (long)a.x,
+                          (long)a.x_lo, a.ld_x, a.epi, (long)a.out, (long)a.out_lo, a.ld_out,
+                          a.permute, a.m_written, a.tail_lo, a.tail_hi, (long)a.w_tail,
+                          a.ld_w_tail, a.tail_row0, a.kchunk, (long)a.status};
+        k.insert(k.end(), std::begin(v), std::end(v));
+    }
+    return k;
+}
+
 // One chain (stage i reads stage i - 1) with its tables in the kernel parameters.
+// A launch with the same operands and shapes as one of the last few reuses its
+// parameter block (tensor maps, stage table, schedule), changing only the
+// counters and the trace buffer.
 template <int OP>
 static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, int *status,
                                    unsigned long long *trace, int num_sms, cudaStream_t s)
 {
     using G = PairGeo<OP>;
     if (n > kChainMaxStages) return cudaErrorNotSupported;
-    static std::mutex mu;  // P (~28 KB) is static: one launch is built at a time
+    static std::mutex mu;  // parameter blocks (~28 KB each) are shared: one launch at a time
     std::lock_guard<std::mutex> lk(mu);
-    static ChainParams P;
+    struct Built {
+        std::vector<long> key;
+        ChainParams P;
+    };
+    static std::vector<Built *> built;  // most recently used last, at most kBuiltKept
+    constexpr size_t kBuiltKept = 8;
+    int device = 0;
+    cudaGetDevice(&device);
+    std::vector<long> pkey = params_key(stages, n, device, num_sms);
+    for (size_t j = 0; j < built.size(); ++j)
+        if (built[j]->key == pkey) {
+            Built *b = built[j];
+            built.erase(built.begin() + j);
+            built.push_back(b);
+            b->P.done = done;
+            b->P.status = status;
+            b->P.trace = trace;
+            return launch_pairs<OP, false>(b->P, b->P.npairs, s);
+        }
+    std::unique_ptr<Built> slot;  // back into `built` once complete; freed on an early return
+    if (built.size() >= kBuiltKept) {
+        slot.reset(built.front());
+        built.erase(built.begin());
+    } else {
+        slot.reset(new Built);
+    }
+    slot->key.clear();
+    ChainParams &P = slot->P;
     memset(&P, 0, sizeof P);
     std::vector<ChainStage> st(n);
     long items = 0;
@@ -604,6 +664,7 @@ static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, in
     struct Cached {
         std::vector<long> key;
         unsigned stream;  // stage boundaries that stream
+        Feeders feed;     // feeder workers of the chosen schedule (none: stage -1)
         std::vector<int> off;
         std::vector<uint32_t> items;
     };
@@ -632,11 +693,38 @@ static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, in
         if (n > 1 && mode != 0u) {
             const unsigned mask = mode == kStreamAuto ? 0xffu : mode;
             set_counters(st, mask);
-            list_schedule(sched_stages(st, G::BK).data(), n, pairs, 2.0, off_s, ent_s, &span_stream);
+            const std::vector<SchedStage> ss = sched_stages(st, G::BK);
+            list_schedule(ss.data(), n, pairs, 2.0, off_s, ent_s, &span_stream);
+            // feeders at a streamed boundary (see Feeders): the best of a small grid
+            if (feed_mode()) {
+                Feeders best;
+                double span_best = span_stream;
+                std::vector<int> off_f;
+                std::vector<WorkEntry> ent_f;
+                for (int f = 0; f + 1 < n; ++f) {
+                    if (!((mask >> f) & 1u)) continue;
+                    for (int q = 2; q <= pairs / 4; q += 2)
+                        for (int d = 1; d <= std::min(8, st[f].tiles_m - 1); ++d) {
+                            Feeders fd;
+                            fd.stage = f;
+                            fd.workers = q;
+                            fd.rows = d;
+                            double span_f = 0.0;
+                            list_schedule(ss.data(), n, pairs, 2.0, off_f, ent_f, &span_f, nullptr, &fd);
+                            if (span_f < span_best - 1e-9) span_best = span_f, best = fd;
+                        }
+                }
+                if (best.stage >= 0 && span_best < 0.99 * span_stream) {
+                    list_schedule(ss.data(), n, pairs, 2.0, off_s, ent_s, &span_stream, nullptr, &best);
+                    c.feed = best;
+                }
+            }
             if (mode != kStreamAuto || span_stream < 0.99 * span_block) {
                 c.stream = mask;
                 c.off.swap(off_s);
                 ent.swap(ent_s);
+            } else {
+                c.feed = Feeders();
             }
         }
         for (const WorkEntry &w : ent)
@@ -649,6 +737,8 @@ static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, in
     for (int i = 0; i < n; ++i) P.st[i] = st[i];
     for (int p = 0; p <= pairs; ++p) P.sched_off[p] = sc->off[p];
     memcpy(P.sched, sc->items.data(), sc->items.size() * sizeof(uint32_t));
+    slot->key.swap(pkey);
+    built.push_back(slot.release());
     return launch_pairs<OP, false>(P, pairs, s);
 }
 

@@ -20,6 +20,8 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include <cstdio>
 #include <cstdlib>
 
@@ -641,14 +643,21 @@ static cudaError_t launch_op(const StageArgs &a, int num_sms, cudaStream_t s)
         twl = tw;
         txl = tx;
     }
-    static unsigned long long attr_set = 0;  // bit per device: the attribute is per context
+    // bit per device: the attribute is per context. Set under a lock, since
+    // callers on several host threads (the allocation-free entry point takes no
+    // library lock) may reach here at once.
+    static std::mutex attr_mu;
+    static unsigned long long attr_set = 0;
     int dev = 0;
     cudaGetDevice(&dev);
-    if (!(attr_set & (1ull << (dev & 63)))) {
-        cudaError_t e = cudaFuncSetAttribute(tc_stage_kernel<OP>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES);
-        if (e != cudaSuccess) return e;
-        attr_set |= 1ull << (dev & 63);
+    {
+        std::lock_guard<std::mutex> lk(attr_mu);
+        if (!(attr_set & (1ull << (dev & 63)))) {
+            cudaError_t e = cudaFuncSetAttribute(
+                tc_stage_kernel<OP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES);
+            if (e != cudaSuccess) return e;
+            attr_set |= 1ull << (dev & 63);
+        }
     }
     const int tiles = ((a.M + kBM - 1) / kBM) * ((a.N + T::BN - 1) / T::BN);
     const int grid = tiles < num_sms ? tiles : num_sms;
@@ -689,6 +698,9 @@ static cudaError_t launch_pair(const StageArgs &a, int num_sms, cudaStream_t s)
     } else {
         twt = tw;
     }
+    // Per device, once, under a lock (see launch_op): the shared-memory attribute
+    // and the occupancy-derived pair count, published together.
+    static std::mutex attr_mu;
     static unsigned long long attr_set = 0;
     static int max_pairs[64];
     int dev = 0;
@@ -704,22 +716,27 @@ static cudaError_t launch_pair(const StageArgs &a, int num_sms, cudaStream_t s)
     cfg.stream = s;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (!(attr_set & (1ull << (dev & 63)))) {
-        cudaError_t e = cudaFuncSetAttribute(tc_pair_kernel<OP>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES);
-        if (e != cudaSuccess) return e;
-        int clusters = 0;
-        cfg.gridDim = dim3(2 * (num_sms / 2));
-        e = cudaOccupancyMaxActiveClusters(&clusters, tc_pair_kernel<OP>, &cfg);
-        if (e != cudaSuccess || clusters < 1) {
-            cudaGetLastError();
-            clusters = num_sms / 2;
+    int cap = 0;
+    {
+        std::lock_guard<std::mutex> lk(attr_mu);
+        if (!(attr_set & (1ull << (dev & 63)))) {
+            cudaError_t e = cudaFuncSetAttribute(
+                tc_pair_kernel<OP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES);
+            if (e != cudaSuccess) return e;
+            int clusters = 0;
+            cfg.gridDim = dim3(2 * (num_sms / 2));
+            e = cudaOccupancyMaxActiveClusters(&clusters, tc_pair_kernel<OP>, &cfg);
+            if (e != cudaSuccess || clusters < 1) {
+                cudaGetLastError();
+                clusters = num_sms / 2;
+            }
+            max_pairs[dev & 63] = clusters;
+            attr_set |= 1ull << (dev & 63);
         }
-        max_pairs[dev & 63] = clusters;
-        attr_set |= 1ull << (dev & 63);
+        cap = max_pairs[dev & 63];
     }
     const int tiles = ((a.M + G::BM - 1) / G::BM) * ((a.N + G::BN - 1) / G::BN);
-    const int pairs = tiles < max_pairs[dev & 63] ? tiles : max_pairs[dev & 63];
+    const int pairs = tiles < cap ? tiles : cap;
     cfg.gridDim = dim3(2 * pairs);
     StageArgs b = a;
     CUtensorMap to;

@@ -553,8 +553,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
 // ------------------------------------------------------------------ scheduling (host)
 
 void list_schedule(const SchedStage *st, int n, int units, double handoff, std::vector<int> &off,
-                   std::vector<WorkEntry> &entries, double *makespan, std::vector<double> *starts)
+                   std::vector<WorkEntry> &entries, double *makespan, std::vector<double> *starts,
+                   const Feeders *feed)
 {
+    const bool feeding = feed && feed->stage >= 0 && feed->stage < n && feed->workers > 0 &&
+                         feed->workers < units && feed->rows > 0;
     double span = 0.0;
     std::vector<int> depth(n, 0), order(n);
     long total = 0, nblocks = 0;
@@ -573,7 +576,7 @@ void list_schedule(const SchedStage *st, int n, int units, double handoff, std::
     // the lowest index. Larger ones: a heap of (free time, worker), O(log workers)
     // per tile; a tile whose input is not ready before the earliest free worker
     // takes that worker.
-    const bool scan = (double)units * (double)total <= 2e5;
+    const bool scan = feeding || (double)units * (double)total <= 2e5;
     std::vector<double> free_at(units, 0.0);
     using Slot = std::pair<double, int>;
     std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
@@ -582,9 +585,30 @@ void list_schedule(const SchedStage *st, int n, int units, double handoff, std::
     for (int si : order) {
         const SchedStage &c = st[si];
         const long count = (long)c.tiles_m * c.tiles_n;
+        // workers [u_lo, u_hi) may take this stage's tiles (feeders: see Feeders)
+        const bool fed = feeding && si == feed->stage;
+        const bool reads_fed = feeding && c.prev == feed->stage;
+        const int defer = fed ? std::min(feed->rows, c.tiles_m) : 0;
+        const long deferred = (long)defer * c.tiles_n;
         for (long it = 0; it < count; ++it) {
-            const int nb = (int)(c.row_major ? it % c.tiles_n : it / c.tiles_m);
-            const int mb = (int)(c.row_major ? it / c.tiles_n : it % c.tiles_m);
+            int nb, mb, u_lo = 0, u_hi = units;
+            if (fed && it >= count - deferred) {
+                // the deferred rows, row tile by row tile, on the feeders only
+                const long k = it - (count - deferred);
+                mb = c.tiles_m - defer + (int)(k / c.tiles_n);
+                nb = (int)(k % c.tiles_n);
+                u_lo = units - feed->workers;
+            } else if (fed) {
+                // the other rows on the other workers, in the stage's own order
+                const int kept = c.tiles_m - defer;
+                nb = (int)(c.row_major ? it % c.tiles_n : it / kept);
+                mb = (int)(c.row_major ? it / c.tiles_n : it % kept);
+                u_hi = units - feed->workers;
+            } else {
+                nb = (int)(c.row_major ? it % c.tiles_n : it / c.tiles_m);
+                mb = (int)(c.row_major ? it / c.tiles_n : it % c.tiles_m);
+                if (reads_fed) u_hi = units - feed->workers;
+            }
                 double ready = 0.0;
                 if (c.prev >= 0) {
                     const SchedStage &p = st[c.prev];
@@ -596,11 +620,11 @@ void list_schedule(const SchedStage *st, int n, int units, double handoff, std::
                             ready = std::max(ready, rd[g] + handoff - (c.stream > 0 ? g * c.stream : 0.0));
                     }
                 }
-                int best = 0;
+                int best = u_lo;
                 double start;
                 if (scan) {
                     start = 1e300;
-                    for (int u = 0; u < units; ++u) {
+                    for (int u = u_lo; u < u_hi; ++u) {
                         const double t = free_at[u] > ready ? free_at[u] : ready;
                         if (t < start - 1e-9) start = t, best = u;
                     }

@@ -535,6 +535,8 @@ FG_EXPORT int fg_chain_group(int dtype, int nchains, const fg_chain_desc *chains
     const int algo = dtype == FG_DT_F32 ? f32_algo() : 0;
     int kernel, order;
     resolved_config(c, dtype, algo, nchains, chains, kernel, order);
+    // everything runs on the caller's stream, after all earlier library work
+    if ((st = enter_stream(c, user_stream(stream)))) return st;
     if ((st = arena_reserve(c, group_buf_bytes(dtype, algo, nchains, chains)))) return st;
     Carver cb;
     cb.base = c->arena;
@@ -544,10 +546,8 @@ FG_EXPORT int fg_chain_group(int dtype, int nchains, const fg_chain_desc *chains
     Carver ct;
     ct.base = c->tab;
     group_place(gx, ct);
-    if ((st = fence_in(c, stream))) return st;
-    if ((st = group_upload(gx, c->stream, false))) return st;
-    if ((st = group_launch(c, gx, c->stream, false))) return st;
-    if ((st = fence_out(c, stream))) return st;
+    if ((st = group_upload(gx, c->work, false))) return st;
+    if ((st = group_launch(c, gx, c->work, false))) return st;
     return ok();
 }
 

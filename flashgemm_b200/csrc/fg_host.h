@@ -65,7 +65,12 @@ inline bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
 struct DevCtx {
     int dev = -1;
     int sms = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;  // the library's own stream (host-pointer calls)
+    // The stream the library's work currently goes to: the caller's stream for
+    // device-pointer calls, the own stream for host-pointer calls. All of the
+    // library's earlier work on this device is ordered before its tail (see
+    // enter_stream), so waiting for it waits for everything the library issued.
+    cudaStream_t work = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     // host-pointer chains: uploads and downloads on their own streams, so that the
     // copies of one column chunk overlap the compute of another
@@ -80,6 +85,11 @@ struct DevCtx {
     size_t tab_cap = 0;
     int *status = nullptr;       // device word the kernels report into
     int *status_host = nullptr;  // pinned copy
+    // Fused-chain dependency counters: a block zeroed once and carved call after
+    // call (every launch gets counters no earlier launch touched), zeroed again in
+    // stream order only when it is used up, instead of a memset per call.
+    int *ctr = nullptr;
+    size_t ctr_cap = 0, ctr_off = 0;
     // per-launch device timing (fg_profile_begin / fg_profile_query)
     struct Rec {
         cudaEvent_t a, b;
@@ -128,7 +138,7 @@ inline double gemm_flops(long M, long N, long K) { return 2.0 * (double)M * (dou
 int launch(cudaError_t e, const char *what);
 
 // Launch one kernel through `fn`; while profiling is on, bracket it with CUDA
-// events on the library's stream (the stream the kernel runs on).
+// events on the stream the kernel runs on.
 template <class Fn>
 int run_kernel_on(DevCtx *c, cudaStream_t stream, bool capturing, int kind, double flops,
                   const char *what, Fn &&fn)
@@ -168,11 +178,11 @@ int run_kernel(DevCtx *c, int kind, double flops, const char *what, Fn &&fn)
             CUDA_TRY(cudaEventCreate(&r.a));
             CUDA_TRY(cudaEventCreate(&r.b));
         }
-        CUDA_TRY(cudaEventRecord(r.a, c->stream));
+        CUDA_TRY(cudaEventRecord(r.a, c->work));
     }
     const int st = launch(fn(), what);
     if (prof) {
-        CUDA_TRY(cudaEventRecord(r.b, c->stream));
+        CUDA_TRY(cudaEventRecord(r.b, c->work));
         c->prof.push_back(r);
     }
     return st;
@@ -197,11 +207,18 @@ int build_tc_stages(DevCtx *c, int dtype, int sem, void *C, long ldc, Mat b, lon
                     const Mat *a, const long *M, const long *K, const PreparedW *pw,
                     std::vector<StageArgs> &out, Carver *cv = nullptr);
 
-// Read and clear the device status word (waits for the context's stream).
+// Read and clear the device status word (waits for the context's work stream).
 int collect_status(DevCtx *c);
 // Order the library's stream after `user` on entry, and `user` after it on exit.
 int fence_in(DevCtx *c, void *user);
 int fence_out(DevCtx *c, void *user);
+// Make `s` the work stream: when it differs from the current one, `s` first
+// waits (event) for everything issued on the current one. A null `user`
+// handle is the legacy default stream.
+int enter_stream(DevCtx *c, cudaStream_t s);
+inline cudaStream_t user_stream(void *user) { return user ? (cudaStream_t)user : cudaStreamLegacy; }
+// `n` zeroed counters for one fused launch on the work stream.
+int take_counters(DevCtx *c, size_t n, int **out);
 
 PreparedW prepared_of(const fg_weights_s *w);
 

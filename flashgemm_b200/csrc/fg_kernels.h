@@ -95,9 +95,21 @@ struct SchedStage {
 // unfinished entry always heads its worker's list and no worker waits forever.
 // makespan (optional): the estimated finish time of the last tile.
 // starts (optional): each entry's estimated start, in the order of `entries`.
+//
+// Feeders (optional): the last `workers` workers take the last `rows` row tiles
+// of every column block of stage `stage` (row tile by row tile, after that
+// stage's other tiles, which they do not take) and no tile of the stage that
+// reads it. The readers, streamed, start on a column block while the feeders
+// still produce its last rows, instead of all waiting for the whole stage.
+// Every worker's list stays in stage order, so no worker waits forever.
+struct Feeders {
+    int stage = -1;  // -1: none
+    int workers = 0;
+    int rows = 0;
+};
 void list_schedule(const SchedStage *st, int n, int units, double handoff, std::vector<int> &off,
                    std::vector<WorkEntry> &entries, double *makespan = nullptr,
-                   std::vector<double> *starts = nullptr);
+                   std::vector<double> *starts = nullptr, const Feeders *feed = nullptr);
 
 enum GroupKernel : int {
     GK_PAIR = 0,        // BF16 / INT8: CTA pairs, 256 x 256 tiles, 6-stage ring

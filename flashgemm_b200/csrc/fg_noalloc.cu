@@ -14,8 +14,11 @@
 // that loads the library, until the process exits. All calls on a device share
 // it and it keeps the last call's contents, so two calls whose kernels overlap
 // on the GPU (different streams, or different host threads without ordering)
-// race on it; the caller orders them. The words that must start at zero (the
-// kernel status word) are cleared by every call.
+// race on it; the caller orders them. Nothing in the array needs to start at
+// zero: the between-stage buffers are written before they are read, and the
+// array's status word (used when the caller passes status == NULL) is zero at
+// load, only ever set by a kernel whose pipeline wait ran out, and read and
+// cleared by fg_sync() (fg_noalloc_take_status below).
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -75,6 +78,30 @@ inline long round_up(long x, long a) { return (x + a - 1) / a * a; }
 
 }  // namespace
 
+namespace fg {
+// Read and clear the array's status word on the current device, where this
+// entry point has run on it (else 0). Synchronous copies on the legacy default
+// stream: the caller has waited for the stream its chains ran on. Used by
+// fg_sync(), so that a time-out of a call made with status == NULL is reported.
+int noalloc_take_status(int dev, int *code)
+{
+    *code = 0;
+    if (dev < 0 || dev >= 64) return 0;
+    char *base;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        base = g_dev[dev].base;
+    }
+    if (!base) return 0;
+    int v = 0;
+    cudaError_t e = cudaMemcpy(&v, base, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && v != 0) e = cudaMemset(base, 0, sizeof(int));
+    if (e != cudaSuccess) return (int)e;
+    *code = v;
+    return 0;
+}
+}  // namespace fg
+
 extern "C" __attribute__((visibility("default"))) int fg_chain_bf16_noalloc(
     float *C, const uint16_t *B, long N, int num_gemm, const uint16_t *const *A, const long *M,
     const long *K, int *status, void *stream)
@@ -85,6 +112,7 @@ extern "C" __attribute__((visibility("default"))) int fg_chain_bf16_noalloc(
         return fg::api_fail(FG_ERR_INVALID, "num_gemm must be in [1, 64]");
     if (N <= 0 || N % 8)
         return fg::api_fail(FG_ERR_INVALID, "N must be a positive multiple of 8 (16-byte rows)");
+    if (N > (1l << 30)) return fg::api_fail(FG_ERR_INVALID, "N must be at most 2^30");
     if (((uintptr_t)C | (uintptr_t)B) & 15)
         return fg::api_fail(FG_ERR_INVALID, "B and C must be 16-byte aligned device pointers");
     for (int i = 0; i < num_gemm; ++i) {
@@ -129,11 +157,10 @@ extern "C" __attribute__((visibility("default"))) int fg_chain_bf16_noalloc(
     if (st) return st;
 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // status == NULL: the array's own word (zero at load; kernels only ever set
+    // it, first time-out wins), kept until fg_sync() reads and clears it, so a
+    // later call cannot erase an earlier call's time-out
     int *kstatus = status ? status : reinterpret_cast<int *>(d.base);
-    if (!status) {
-        e = cudaMemsetAsync(kstatus, 0, sizeof(int), s);
-        if (e != cudaSuccess) return fg::api_fail(FG_ERR_CUDA, cudaGetErrorString(e));
-    }
     uint16_t *buf[2] = {reinterpret_cast<uint16_t *>(d.base + kHeaderBytes),
                         reinterpret_cast<uint16_t *>(d.base + kHeaderBytes + region[0])};
 

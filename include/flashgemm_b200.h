@@ -252,7 +252,9 @@ int fg_server_reset_stats(fg_server s);
 int fg_server_destroy(fg_server s);
 
 /* Wait for all of the library's work on the current device and report any
- * kernel-side error since the last fg_sync (then cleared). */
+ * kernel-side error since the last fg_sync (then cleared). This includes a
+ * time-out of a fg_chain_bf16_noalloc call made with status == NULL, once the
+ * caller's stream has finished that call. */
 int fg_sync(void);
 
 /* Number of kernels this library has launched in this process (all devices).
@@ -302,7 +304,10 @@ int fg_profile_query(int kind, double *total_ms, unsigned long long *launches, d
  * contents: calls whose kernels overlap on the GPU race, so order them (one
  * stream, or events). `status`, if not NULL, is a device int the kernels set
  * to a nonzero code when a bounded pipeline wait runs out (the caller clears
- * it); with NULL the kernels use a word of the array that every call clears.
+ * it). With NULL they set a word of the array instead, which is zero at load
+ * and stays set until fg_sync() reports it as FG_ERR_TIMEOUT and clears it
+ * (after the caller's stream has finished the call); the call itself returns
+ * before its kernels run, so it cannot report a time-out in its return code.
  * The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) and the SM count; make that first call before any
  * stream capture. Returns a fg_status; the message is in fg_last_error(). */
