@@ -711,7 +711,8 @@ def run_serve(args, world, rank, local_rank, g=None):
                           "50% BF16 / 30% INT8 / 20% FP32 (3xTF32) over 64 resident weight sets; "
                           "activations and results resident in HBM",
               "requests_per_rate": nreq, "weight_sets": len(sets),
-              "server": {"max_batch": 64, "slots": 2, "max_wait_us": 200},
+              "server": {"max_batch": 64, "slots": 2, "max_wait_us": 200,
+                         "max_queue_us": args.serve_deadline_us},
               "l2": "inputs of the stream far exceed L2; no flush between requests",
               "parallelism": f"dp{world} (each rank serves its own stream)"}
     metric = "served chain requests TFLOP/s (p50/p99 latency beside)"
@@ -772,7 +773,7 @@ def run_serve(args, world, rank, local_rank, g=None):
             out.append((dt, W[i], Bs[i][:K1 * N].view(K1, N), c[:Ms[-1] * N].view(Ms[-1], N)))
         return out
 
-    srv = fg.Server(max_batch=64, slots=2, max_wait_us=200)
+    srv = fg.Server(max_batch=64, slots=2, max_wait_us=200, max_queue_us=args.serve_deadline_us)
 
     def run_point(reqs, at_us, prof=False):
         if dist:
@@ -795,7 +796,7 @@ def run_serve(args, world, rank, local_rank, g=None):
             fg.profile_end()
         launches = fg.kernel_launches() - l0
         for rid in ids:
-            srv.wait(rid)
+            srv.wait(rid, shed_ok=True)
         return st, launches, kernels, sum(fl)
 
     # warm-up (memory pool at full batch size, tensor-map encoder, code paths), then
@@ -817,7 +818,8 @@ def run_serve(args, world, rank, local_rank, g=None):
             rate = frac * capacity
             reqs = serve_requests(seed + 10 + k, sets, nreq)
             at = np.cumsum(rng.exponential(1e6 / rate, size=nreq))
-            prof = k == len(args.serve_rates) - 1
+            under = [f for f in args.serve_rates if f <= 1.0] or args.serve_rates
+            prof = frac == max(under)  # kernel times at the headline point
             st, launches, kern, fl = run_point(reqs, at.tolist(), prof=prof)
             launches_total += launches
             if prof:
@@ -828,7 +830,9 @@ def run_serve(args, world, rank, local_rank, g=None):
                            "p50_us": st["p50_us"], "p99_us": st["p99_us"],
                            "mean_us": st["mean_us"], "max_us": st["max_us"],
                            "batches": st["batches"], "mean_batch": st["mean_batch"],
-                           "failed": st["failed"], "peak_bytes": st["peak_bytes"]})
+                           "failed": st["failed"], "shed": st["shed"],
+                           "shed_frac": st["shed"] / max(1, st["submitted"]),
+                           "peak_bytes": st["peak_bytes"]})
 
     # end to end: host (pinned) activations in and results out inside each request
     e2e_n = min(nreq, 4000)
@@ -853,15 +857,19 @@ def run_serve(args, world, rank, local_rank, g=None):
     srv.drain()
     st_e2e = srv.stats()
     for rid in ids:
-        srv.wait(rid)
+        srv.wait(rid, shed_ok=True)
     srv.close()
     for ws in W:
         for w in ws:
             w.release()
+    # the headline point: the highest offered rate at or below the measured capacity
+    # (points above it show the shedding that keeps served latency bounded)
+    sustained = [p for p in points if p["offered_frac_of_capacity"] <= 1.0] or points
+    top = max(sustained, key=lambda p: p["offered_frac_of_capacity"])
     # whole job: throughput summed over the ranks' streams, latency the worst rank's
-    job_tflops = points[-1]["tflops"]
+    job_tflops = top["tflops"]
     job_e2e = st_e2e["flops"] / st_e2e["span_s"] / 1e12
-    lat = [points[-1]["p50_us"], points[-1]["p99_us"]]
+    lat = [top["p50_us"], top["p99_us"]]
     if dist:
         t = torch.tensor([job_tflops, job_e2e], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
@@ -873,7 +881,6 @@ def run_serve(args, world, rank, local_rank, g=None):
     if rank != 0:
         return None
 
-    top = points[-1]
     peaks, peak_src = load_peaks()
     main = max(kernels.items(), key=lambda kv: kv[1][0]) if kernels else None
     roofline = None
@@ -1288,6 +1295,8 @@ def main():
     ap.add_argument("--serve-rates", type=float, nargs="+", default=None,
                     help="serve: offered rates as fractions of the measured capacity "
                          "(default 0.3 0.6 0.9; 0.6 within 'all')")
+    ap.add_argument("--serve-deadline-us", type=int, default=20000,
+                    help="serve: the server sheds requests still queued this long after submit")
     ap.add_argument("--e2e-steps", type=int, default=None,
                     help="steps of the host-buffer C-ABI measurement (default: min(steps, 200))")
     ap.add_argument("--cpu-budget", type=float, default=None,
@@ -1305,7 +1314,7 @@ def main():
     if args.serve_requests is None:
         args.serve_requests = 4000 if combined else 20000
     if args.serve_rates is None:
-        args.serve_rates = [0.6] if combined else [0.3, 0.6, 0.9]
+        args.serve_rates = [0.6, 1.2] if combined else [0.3, 0.6, 0.9, 1.2]
     if args.cpu_budget is None:
         args.cpu_budget = 6.0 if combined else 12.0
 

@@ -25,7 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libflashgemm_b200.so")
 
 FG_OK, FG_ERR_INVALID, FG_ERR_UNSUPPORTED, FG_ERR_CUDA, FG_ERR_NO_DEVICE, FG_ERR_TIMEOUT, \
-    FG_ERR_NOMEM = range(7)
+    FG_ERR_NOMEM, FG_ERR_BUSY = range(8)
 FG_SEM_REF, FG_SEM_MATH = 0, 1
 FG_F32_FFMA, FG_F32_3XTF32 = 0, 1
 FG_DT_F32, FG_DT_BF16, FG_DT_INT8 = 0, 1, 2
@@ -123,6 +123,14 @@ def sync():
     st = lib().fg_sync()
     if st != FG_OK:
         raise FlashgemmError(st, last_error())
+
+
+def selftest_timeout(limit_us=2000):
+    """Run the failure-detection self-test (fg_selftest_timeout): a fused chain
+    whose second stage waits on a dependency nothing releases, its waits
+    limited to limit_us. Returns the status the host read (FG_ERR_TIMEOUT when
+    detection works); raises nothing."""
+    return lib().fg_selftest_timeout(int(limit_us))
 
 
 # ------------------------------------------------------------ reference entry points
@@ -469,12 +477,13 @@ class _Request(ctypes.Structure):
 class _ServerOpts(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_longlong), ("max_batch", ctypes.c_int),
                 ("slots", ctypes.c_int), ("max_wait_us", ctypes.c_int),
-                ("ctas_per_batch", ctypes.c_int)]
+                ("ctas_per_batch", ctypes.c_int), ("max_queue_us", ctypes.c_int)]
 
 
 class _ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
-                ("failed", ctypes.c_longlong), ("batches", ctypes.c_longlong),
+                ("failed", ctypes.c_longlong), ("shed", ctypes.c_longlong),
+                ("batches", ctypes.c_longlong),
                 ("mean_batch", ctypes.c_double), ("p50_us", ctypes.c_double),
                 ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double),
                 ("max_us", ctypes.c_double), ("flops", ctypes.c_double),
@@ -485,7 +494,8 @@ class Server:
     """The library's request loop (fg_server_*): chain requests on registered
     weights, admitted by device memory, batched into grouped launches."""
 
-    def __init__(self, hbm_budget=0, max_batch=0, slots=0, max_wait_us=0, ctas_per_batch=0):
+    def __init__(self, hbm_budget=0, max_batch=0, slots=0, max_wait_us=0, ctas_per_batch=0,
+                 max_queue_us=0):
         L = lib()
         L.fg_server_create.argtypes = [_P, _P]
         L.fg_server_submit.argtypes = [_P, _P]
@@ -496,7 +506,7 @@ class Server:
         L.fg_server_reset_stats.argtypes = [_P]
         L.fg_server_destroy.argtypes = [_P]
         o = _ServerOpts(int(hbm_budget), int(max_batch), int(slots), int(max_wait_us),
-                        int(ctas_per_batch))
+                        int(ctas_per_batch), int(max_queue_us))
         h = _P()
         st = L.fg_server_create(ctypes.byref(o), ctypes.byref(h))
         if st != FG_OK:
@@ -520,12 +530,16 @@ class Server:
         self._keep[rid] = (hs, B, C, weights)
         return rid
 
-    def wait(self, rid):
-        """Blocks until request `rid` is done; returns its latency in microseconds."""
+    def wait(self, rid, shed_ok=False):
+        """Blocks until request `rid` is done; returns its latency in microseconds.
+        shed_ok: a request shed under load (FG_ERR_BUSY) returns None instead of
+        raising."""
         L = lib()
         lat = ctypes.c_double()
         st = L.fg_server_wait(self.handle, ctypes.c_longlong(rid), ctypes.byref(lat))
         self._keep.pop(rid, None)
+        if st == FG_ERR_BUSY and shed_ok:
+            return None
         if st != FG_OK:
             raise FlashgemmError(st, last_error())
         return lat.value

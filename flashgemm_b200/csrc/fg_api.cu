@@ -601,6 +601,47 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
             });
             if (st) return st;
         }
+        if (fused_enabled() && panel_enabled() && panel_eligible(N, n, M, K) &&
+            aligned16(b.p) && aligned16(C) && b.ld % 4 == 0 && ldc % 4 == 0) {
+            // every dimension fits on chip: one launch, intermediates in shared memory
+            PanelChainArgs pa;
+            memset(&pa, 0, sizeof pa);
+            pa.n = n;
+            pa.N = N;
+            pa.B = (const float *)b.p;
+            pa.ldb = b.ld;
+            pa.C = (float *)C;
+            pa.ldc = ldc;
+            for (int i = 0; i < n; ++i) {
+                pa.w_hi[i] = wh[i];
+                pa.w_lo[i] = wl[i];
+                pa.ldw[i] = wld[i];
+                pa.M[i] = M[i];
+                pa.K[i] = K[i];
+                pa.kchunk[i] = tf32_chunk_blocks(K[i]);
+            }
+            GroupExec gx;
+            gx.panel.resize(1);
+            cudaError_t e = panel_chain_desc(pa, gx.panel[0]);
+            if (e != cudaSuccess) return fail(FG_ERR_INVALID, "panel tables: %s", cudaGetErrorString(e));
+            double fl = 0.0;
+            for (int i = 0; i < n; ++i) fl += gemm_flops(M[i], N, K[i]);
+            int st = panel_finish(c, gx);
+            if (st) return st;
+            PanelChain *pd = (PanelChain *)arena_take(c, sizeof(PanelChain));
+            uint32_t *bd = (uint32_t *)arena_take(c, gx.panel_blocks.size() * sizeof(uint32_t));
+            int *od = (int *)arena_take(c, gx.panel_off.size() * sizeof(int));
+            CUDA_TRY(cudaMemcpyAsync(pd, gx.panel.data(), sizeof(PanelChain), cudaMemcpyHostToDevice,
+                                     c->work));
+            CUDA_TRY(cudaMemcpyAsync(bd, gx.panel_blocks.data(),
+                                     gx.panel_blocks.size() * sizeof(uint32_t),
+                                     cudaMemcpyHostToDevice, c->work));
+            CUDA_TRY(cudaMemcpyAsync(od, gx.panel_off.data(), gx.panel_off.size() * sizeof(int),
+                                     cudaMemcpyHostToDevice, c->work));
+            return run_kernel(c, FG_PK_TC_TF32X3, fl, "panel-resident chain", [&] {
+                return launch_panel(pd, bd, od, gx.panel_ctas, c->status, c->work);
+            });
+        }
         float *xh = (float *)arena_take(c, (size_t)K[0] * ldN * 4);
         float *xl = (float *)arena_take(c, (size_t)K[0] * ldN * 4);
         int st = run_kernel(c, FG_PK_AUX, 0.0, "tf32 split (activations)", [&] {
@@ -1192,6 +1233,42 @@ FG_EXPORT int fg_sync(void)
         return fail(FG_ERR_TIMEOUT, "fg_chain_bf16_noalloc: a kernel's pipeline wait ran out "
                                     "(code 0x%x)", code);
     return ok();
+}
+
+FG_EXPORT int fg_selftest_timeout(int limit_us)
+{
+    if (limit_us < 100 || limit_us > 1000000)
+        return fail(FG_ERR_INVALID, "limit_us must be in [100, 1000000]");
+    DevCtx *c;
+    int st;
+    if ((st = get_ctx(&c))) return st;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if ((st = enter_stream(c, c->stream))) return st;
+    // a small BF16 chain: B 64 x 512, A1 256 x 64, A2 128 x 256 (values irrelevant)
+    const long N = 512, K1 = 64;
+    const long M[2] = {256, 128}, K[2] = {K1, 256};
+    const size_t need = carve_size((size_t)K1 * N * 2) + carve_size((size_t)M[0] * K[0] * 2) +
+                        carve_size((size_t)M[1] * K[1] * 2) + carve_size((size_t)M[1] * N * 4) +
+                        chain_scratch(FG_DT_BF16, 0, N, 2, M, K) + 4096;
+    if ((st = arena_reserve(c, need))) return st;
+    void *b = arena_take(c, (size_t)K1 * N * 2);
+    void *a0 = arena_take(c, (size_t)M[0] * K[0] * 2);
+    void *a1 = arena_take(c, (size_t)M[1] * K[1] * 2);
+    void *cc = arena_take(c, (size_t)M[1] * N * 4);
+    CUDA_TRY(cudaMemsetAsync(c->arena, 0, c->arena_off, c->stream));
+    const Mat a[2] = {{a0, K[0]}, {a1, K[1]}};
+    std::vector<StageArgs> stages;
+    if ((st = build_tc_stages(c, FG_DT_BF16, FG_SEM_REF, cc, N, Mat{b, N}, N, 2, a, M, K,
+                              nullptr, stages)))
+        return st;
+    int *done = nullptr;
+    if ((st = take_counters(c, 3 * chain_counter_ints(2, M, N), &done))) return st;
+    if ((st = launch(launch_tc_chain_stuck(stages.data(), done, c->status, c->sms,
+                                           (unsigned long long)limit_us * 1000ull, c->stream),
+                     "time-out self-test")))
+        return st;
+    // the kernel has returned on its own once this completes
+    return collect_status(c);
 }
 
 FG_EXPORT int fg_profile_begin(void)

@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
                         const uint64_t t0 = globaltimer_ns();
                         while (ld_acquire_gpu(cnt) < need) {
                             __nanosleep(64);
-                            if (globaltimer_ns() - t0 > kWaitLimitNs) {
+                            if (globaltimer_ns() - t0 > wait_limit_ns()) {
                                 atomicCAS(status, 0, KERR_WAIT_DEPENDENCY);
                                 set_abort(bars);
                                 goto producer_done;
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
                             const uint64_t t0 = globaltimer_ns();
                             while (ld_acquire_gpu(row_cnt + g) < kDoneIncrementsPerTile) {
                                 __nanosleep(32);
-                                if (globaltimer_ns() - t0 > kWaitLimitNs) {
+                                if (globaltimer_ns() - t0 > wait_limit_ns()) {
                                     atomicCAS(status, 0, KERR_WAIT_DEPENDENCY);
                                     set_abort(bars);
                                     goto producer_done;
@@ -559,7 +559,19 @@ void set_counters(std::vector<ChainStage> &st, unsigned stream)
 // else none. (Measured on B200: the BF16 chain 4096x1024 -> 4096 -> 1024 ->
 // 1024, estimate 0.978 of block-wise, ran 4 % faster streamed; the INT8 chain
 // 8192x2048 -> 4096 -> 2048 -> 4096 -> 1024, estimate 1.008, 15 % slower.)
-// FG_CHAIN_FEED=0: no feeder workers (see Feeders) in a single chain's schedule;
+// FG_CHAIN_WINDOW=<blocks>: place a single chain's tiles that many 256-column
+// blocks at a time, every stage of them before the next blocks' (SchedOpts);
+// unset or 0: each stage whole.
+int window_blocks()
+{
+    static const int w = [] {
+        const char *v = getenv("FG_CHAIN_WINDOW");
+        return v ? atoi(v) : 0;
+    }();
+    return w > 0 ? w : 0;
+}
+
+// FG_CHAIN_FEED=0: no feeder workers (see SchedOpts) in a single chain's schedule;
 // otherwise the host tries them at every streamed boundary and keeps them when
 // the estimate is at least 1 % shorter.
 bool feed_mode()
@@ -664,7 +676,7 @@ static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, in
     struct Cached {
         std::vector<long> key;
         unsigned stream;  // stage boundaries that stream
-        Feeders feed;     // feeder workers of the chosen schedule (none: stage -1)
+        SchedOpts opts;   // feeders and window of the chosen schedule
         std::vector<int> off;
         std::vector<uint32_t> items;
     };
@@ -686,18 +698,23 @@ static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, in
         double span_block = 0.0, span_stream = 0.0;
         std::vector<int> off_s;
         std::vector<WorkEntry> ent_s;
+        SchedOpts base;
+        base.window = window_blocks();
+        c.opts = base;
         set_counters(st, 0u);
-        list_schedule(sched_stages(st, G::BK).data(), n, pairs, 2.0, c.off, ent, &span_block);
+        list_schedule(sched_stages(st, G::BK).data(), n, pairs, 2.0, c.off, ent, &span_block,
+                      nullptr, &base);
         c.stream = 0u;
         const unsigned mode = stream_mode();
         if (n > 1 && mode != 0u) {
             const unsigned mask = mode == kStreamAuto ? 0xffu : mode;
             set_counters(st, mask);
             const std::vector<SchedStage> ss = sched_stages(st, G::BK);
-            list_schedule(ss.data(), n, pairs, 2.0, off_s, ent_s, &span_stream);
-            // feeders at a streamed boundary (see Feeders): the best of a small grid
+            list_schedule(ss.data(), n, pairs, 2.0, off_s, ent_s, &span_stream, nullptr, &base);
+            // feeders at a streamed boundary (see SchedOpts): the best of a small grid
+            SchedOpts chosen = base;
             if (feed_mode()) {
-                Feeders best;
+                SchedOpts best = base;
                 double span_best = span_stream;
                 std::vector<int> off_f;
                 std::vector<WorkEntry> ent_f;
@@ -705,26 +722,25 @@ static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, in
                     if (!((mask >> f) & 1u)) continue;
                     for (int q = 2; q <= pairs / 4; q += 2)
                         for (int d = 1; d <= std::min(8, st[f].tiles_m - 1); ++d) {
-                            Feeders fd;
-                            fd.stage = f;
-                            fd.workers = q;
-                            fd.rows = d;
+                            SchedOpts fd = base;
+                            fd.feed_stage = f;
+                            fd.feed_workers = q;
+                            fd.feed_rows = d;
                             double span_f = 0.0;
                             list_schedule(ss.data(), n, pairs, 2.0, off_f, ent_f, &span_f, nullptr, &fd);
                             if (span_f < span_best - 1e-9) span_best = span_f, best = fd;
                         }
                 }
-                if (best.stage >= 0 && span_best < 0.99 * span_stream) {
+                if (best.feed_stage >= 0 && span_best < 0.99 * span_stream) {
                     list_schedule(ss.data(), n, pairs, 2.0, off_s, ent_s, &span_stream, nullptr, &best);
-                    c.feed = best;
+                    chosen = best;
                 }
             }
             if (mode != kStreamAuto || span_stream < 0.99 * span_block) {
                 c.stream = mask;
+                c.opts = chosen;
                 c.off.swap(off_s);
                 ent.swap(ent_s);
-            } else {
-                c.feed = Feeders();
             }
         }
         for (const WorkEntry &w : ent)
@@ -740,6 +756,60 @@ static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, in
     slot->key.swap(pkey);
     built.push_back(slot.release());
     return launch_pairs<OP, false>(P, pairs, s);
+}
+
+// Time-out self-test: a BF16 chain of two stages whose second stage waits on
+// column-block counters that no tile releases (those of a third, unlisted copy
+// of the first stage), with every wait of this launch limited to limit_ns.
+// The second stage's producers, its MMA issuer and its epilogue warps run out,
+// record an error code in *status, stop and return; the first stage's tiles
+// complete. The limit is set and restored in stream order around the launch.
+// `done` holds 3 * chain_counter_ints zeroed ints.
+cudaError_t launch_tc_chain_stuck(const StageArgs *stages, int *done, int *status, int num_sms,
+                                  unsigned long long limit_ns, cudaStream_t s)
+{
+    using G = PairGeo<OP_BF16>;
+    if (stages[0].op != OP_BF16 || stages[1].op != OP_BF16) return cudaErrorInvalidValue;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    std::unique_ptr<ChainParams> P(new ChainParams);
+    memset(P.get(), 0, sizeof *P);
+    std::vector<ChainStage> st(2);
+    for (int i = 0; i < 2; ++i) {
+        cudaError_t e = make_chain_stage<OP_BF16>(stages[i], i - 1, 0, st[i]);
+        if (e != cudaSuccess) return e;
+    }
+    set_counters(st, 0u);
+    int pairs = 0;
+    cudaError_t e = pair_capacity<OP_BF16>(num_sms, pairs);
+    if (e != cudaSuccess) return e;
+    const long items = (long)st[0].tiles_m * st[0].tiles_n + (long)st[1].tiles_m * st[1].tiles_n;
+    if (items > kParamSchedItems) return cudaErrorNotSupported;
+    if (items < pairs) pairs = (int)items;
+    std::vector<int> off;
+    std::vector<WorkEntry> ent;
+    list_schedule(sched_stages(st, G::BK).data(), 2, pairs, 2.0, off, ent);
+    P->st[0] = st[0];
+    P->st[1] = st[1];
+    P->st[2] = st[0];  // never listed: its counters are never released
+    P->st[2].done_off = st[1].done_off + st[1].tiles_n;
+    P->st[1].prev = 2;
+    P->npairs = pairs;
+    P->done = done;
+    P->status = status;
+    for (int p = 0; p <= pairs; ++p) P->sched_off[p] = off[p];
+    for (size_t i = 0; i < ent.size(); ++i)
+        P->sched[i] = pack_item((int)ent[i].stage, (int)(ent[i].mbnb >> 16), (int)(ent[i].mbnb & 0xffffu));
+    static const unsigned long long dflt = kWaitLimitNs;
+    static unsigned long long lowered;
+    lowered = limit_ns;
+    e = cudaMemcpyToSymbolAsync(fg_wait_limit_ns, &lowered, sizeof lowered, 0,
+                                cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    e = launch_pairs<OP_BF16, false>(*P, pairs, s);
+    const cudaError_t e2 = cudaMemcpyToSymbolAsync(fg_wait_limit_ns, &dflt, sizeof dflt, 0,
+                                                   cudaMemcpyHostToDevice, s);
+    return e != cudaSuccess ? e : e2;
 }
 
 cudaError_t launch_tc_chain(const StageArgs *stages, int n, int *done, int *status,

@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
                         const uint64_t t0 = globaltimer_ns();
                         while (ld_acquire_gpu(cnt) < need) {
                             __nanosleep(64);
-                            if (globaltimer_ns() - t0 > kWaitLimitNs) {
+                            if (globaltimer_ns() - t0 > wait_limit_ns()) {
                                 atomicCAS(status, 0, KERR_WAIT_DEPENDENCY);
                                 set_abort(bars);
                                 goto producer_done;
@@ -554,97 +554,109 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
 
 void list_schedule(const SchedStage *st, int n, int units, double handoff, std::vector<int> &off,
                    std::vector<WorkEntry> &entries, double *makespan, std::vector<double> *starts,
-                   const Feeders *feed)
+                   const SchedOpts *opts)
 {
-    const bool feeding = feed && feed->stage >= 0 && feed->stage < n && feed->workers > 0 &&
-                         feed->workers < units && feed->rows > 0;
+    SchedOpts o;
+    if (opts) o = *opts;
+    const bool feeding = o.feed_stage >= 0 && o.feed_stage < n && o.feed_workers > 0 &&
+                         o.feed_workers < units && o.feed_rows > 0;
     double span = 0.0;
     std::vector<int> depth(n, 0), order(n);
     long total = 0, nblocks = 0;
+    int max_tn = 0;
     for (int i = 0; i < n; ++i) {
         depth[i] = st[i].prev < 0 ? 0 : depth[st[i].prev] + 1;
         order[i] = i;
         total += (long)st[i].tiles_m * st[i].tiles_n;
+        max_tn = std::max(max_tn, st[i].tiles_n);
         nblocks = std::max<long>(nblocks, (long)st[i].done_off +
                                               (long)st[i].tiles_n * (st[i].row_done ? st[i].tiles_m : 1));
     }
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return depth[x] < depth[y]; });
+
+    // ---- the placement order: windows of column blocks, stages in depth order,
+    // each stage's tiles column block by column block (or row tile by row tile);
+    // a fed stage's deferred rows after its other tiles
+    struct Item {
+        int si, mb, nb;
+        int u_lo, u_hi;  // workers that may take it
+    };
+    std::vector<Item> items;
+    items.reserve(total);
+    const int W = o.window > 0 ? o.window : (max_tn > 0 ? max_tn : 1);
+    for (int w0 = 0; w0 < std::max(max_tn, 1); w0 += W)
+        for (int si : order) {
+            const SchedStage &c = st[si];
+            const int n0 = std::min(w0, c.tiles_n), n1 = std::min(w0 + W, c.tiles_n);
+            const int nw = n1 - n0;
+            if (nw <= 0) continue;
+            const bool fed = feeding && si == o.feed_stage;
+            const bool reads_fed = feeding && c.prev == o.feed_stage;
+            const int defer = fed ? std::min(o.feed_rows, c.tiles_m) : 0;
+            const int kept = c.tiles_m - defer;
+            const int hi = reads_fed || fed ? units - o.feed_workers : units;
+            for (long it = 0; it < (long)kept * nw; ++it) {
+                const int nb = n0 + (int)(c.row_major ? it % nw : it / kept);
+                const int mb = (int)(c.row_major ? it / nw : it % kept);
+                items.push_back(Item{si, mb, nb, 0, hi});
+            }
+            for (long it = 0; it < (long)defer * nw; ++it)  // feeders only
+                items.push_back(Item{si, kept + (int)(it / nw), n0 + (int)(it % nw),
+                                     units - o.feed_workers, units});
+        }
+
+    // ---- placement: each tile to the allowed worker that can start it first
     std::vector<double> block_done(nblocks, 0.0);
     std::vector<std::vector<WorkEntry>> per(units);
     std::vector<std::vector<double>> per_start(starts ? units : 0);
-    // Small problems (one chain's few hundred tiles): scan every worker, ties to
-    // the lowest index. Larger ones: a heap of (free time, worker), O(log workers)
-    // per tile; a tile whose input is not ready before the earliest free worker
-    // takes that worker.
+    // Small problems (one chain's few hundred tiles) or restricted workers: scan
+    // the allowed workers, ties to the lowest index. Larger ones: a heap of (free
+    // time, worker), O(log workers) per tile; a tile whose input is not ready
+    // before the earliest free worker takes that worker.
     const bool scan = feeding || (double)units * (double)total <= 2e5;
     std::vector<double> free_at(units, 0.0);
     using Slot = std::pair<double, int>;
     std::priority_queue<Slot, std::vector<Slot>, std::greater<Slot>> heap;
     if (!scan)
         for (int u = 0; u < units; ++u) heap.push({0.0, u});
-    for (int si : order) {
-        const SchedStage &c = st[si];
-        const long count = (long)c.tiles_m * c.tiles_n;
-        // workers [u_lo, u_hi) may take this stage's tiles (feeders: see Feeders)
-        const bool fed = feeding && si == feed->stage;
-        const bool reads_fed = feeding && c.prev == feed->stage;
-        const int defer = fed ? std::min(feed->rows, c.tiles_m) : 0;
-        const long deferred = (long)defer * c.tiles_n;
-        for (long it = 0; it < count; ++it) {
-            int nb, mb, u_lo = 0, u_hi = units;
-            if (fed && it >= count - deferred) {
-                // the deferred rows, row tile by row tile, on the feeders only
-                const long k = it - (count - deferred);
-                mb = c.tiles_m - defer + (int)(k / c.tiles_n);
-                nb = (int)(k % c.tiles_n);
-                u_lo = units - feed->workers;
-            } else if (fed) {
-                // the other rows on the other workers, in the stage's own order
-                const int kept = c.tiles_m - defer;
-                nb = (int)(c.row_major ? it % c.tiles_n : it / kept);
-                mb = (int)(c.row_major ? it / c.tiles_n : it % kept);
-                u_hi = units - feed->workers;
+    for (const Item &t : items) {
+        const SchedStage &c = st[t.si];
+        const int nb = t.nb, mb = t.mb;
+        double ready = 0.0;
+        if (c.prev >= 0) {
+            const SchedStage &p = st[c.prev];
+            if (!p.row_done) {
+                ready = block_done[p.done_off + nb] + handoff;
             } else {
-                nb = (int)(c.row_major ? it % c.tiles_n : it / c.tiles_m);
-                mb = (int)(c.row_major ? it / c.tiles_n : it % c.tiles_m);
-                if (reads_fed) u_hi = units - feed->workers;
+                const double *rd = &block_done[p.done_off + (long)nb * p.tiles_m];
+                for (int g = 0; g < p.tiles_m; ++g)
+                    ready = std::max(ready, rd[g] + handoff - (c.stream > 0 ? g * c.stream : 0.0));
             }
-                double ready = 0.0;
-                if (c.prev >= 0) {
-                    const SchedStage &p = st[c.prev];
-                    if (!p.row_done) {
-                        ready = block_done[p.done_off + nb] + handoff;
-                    } else {
-                        const double *rd = &block_done[p.done_off + (long)nb * p.tiles_m];
-                        for (int g = 0; g < p.tiles_m; ++g)
-                            ready = std::max(ready, rd[g] + handoff - (c.stream > 0 ? g * c.stream : 0.0));
-                    }
-                }
-                int best = u_lo;
-                double start;
-                if (scan) {
-                    start = 1e300;
-                    for (int u = u_lo; u < u_hi; ++u) {
-                        const double t = free_at[u] > ready ? free_at[u] : ready;
-                        if (t < start - 1e-9) start = t, best = u;
-                    }
-                } else {
-                    const Slot top = heap.top();
-                    heap.pop();
-                    best = top.second;
-                    start = top.first > ready ? top.first : ready;
-                }
-                const double fin = start + c.cost;
-                if (scan)
-                    free_at[best] = fin;
-                else
-                    heap.push({fin, best});
-                per[best].push_back(WorkEntry{(uint32_t)si, ((uint32_t)mb << 16) | (uint32_t)nb});
-                if (starts) per_start[best].push_back(start);
-                double &bd = block_done[c.done_off + (c.row_done ? (long)nb * c.tiles_m + mb : nb)];
-                if (fin > bd) bd = fin;
-                if (fin > span) span = fin;
+        }
+        int best = t.u_lo;
+        double start;
+        if (scan) {
+            start = 1e300;
+            for (int u = t.u_lo; u < t.u_hi; ++u) {
+                const double tu = free_at[u] > ready ? free_at[u] : ready;
+                if (tu < start - 1e-9) start = tu, best = u;
             }
+        } else {
+            const Slot top = heap.top();
+            heap.pop();
+            best = top.second;
+            start = top.first > ready ? top.first : ready;
+        }
+        const double fin = start + c.cost;
+        if (scan)
+            free_at[best] = fin;
+        else
+            heap.push({fin, best});
+        per[best].push_back(WorkEntry{(uint32_t)t.si, ((uint32_t)mb << 16) | (uint32_t)nb});
+        if (starts) per_start[best].push_back(start);
+        double &bd = block_done[c.done_off + (c.row_done ? (long)nb * c.tiles_m + mb : nb)];
+        if (fin > bd) bd = fin;
+        if (fin > span) span = fin;
     }
     if (makespan) *makespan = span;
     off.assign(units + 1, 0);

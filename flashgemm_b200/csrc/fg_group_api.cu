@@ -230,6 +230,36 @@ void group_resolve(DevCtx *c, int dtype, int algo, int nchains, const fg_chain_d
     order = bo;
 }
 
+bool panel_enabled()
+{
+    static const bool on = [] {
+        const char *v = getenv("FG_PANEL");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
+int panel_finish(DevCtx *c, GroupExec &gx, int max_units)
+{
+    if (gx.panel.empty()) return FG_OK;
+    int ctas = 0;
+    cudaError_t e = panel_capacity(max_units > 0 ? max_units : c->sms, ctas);
+    if (e != cudaSuccess) return fail(FG_ERR_CUDA, "panel launch: %s", cudaGetErrorString(e));
+    std::vector<int> cost, nblocks;
+    long total = 0;
+    for (const PanelChain &pc : gx.panel) {
+        int kb = 0;
+        for (int i = 0; i < pc.n; ++i) kb += (pc.K[i] + 31) / 32;
+        cost.push_back(kb);
+        nblocks.push_back(panel_blocks_of(pc.N));
+        total += nblocks.back();
+    }
+    if (total < ctas) ctas = (int)total;
+    panel_plan(cost, nblocks, ctas, gx.panel_blocks, gx.panel_off);
+    gx.panel_ctas = ctas;
+    return FG_OK;
+}
+
 // Host side of a grouped launch: between-stage buffers carved from `cv`, stage
 // lists, schedules and tables (device addresses of the tables come later).
 int group_build(DevCtx *c, int dtype, int algo, int kernel, int order, int nchains,
@@ -288,6 +318,33 @@ int group_build(DevCtx *c, int dtype, int algo, int kernel, int order, int nchai
             continue;
         }
         std::vector<StageArgs> stg;
+        if (dtype == FG_DT_F32 && panel_enabled() && panel_eligible(N, n, M.data(), K.data()) &&
+            gx.panel.size() < 65536) {
+            // intermediates on chip: one panel launch for all such chains
+            PanelChainArgs pa;
+            memset(&pa, 0, sizeof pa);
+            pa.n = n;
+            pa.N = N;
+            pa.B = (const float *)d.B;
+            pa.ldb = N;
+            pa.C = (float *)d.C;
+            pa.ldc = N;
+            for (int i = 0; i < n; ++i) {
+                pa.w_hi[i] = pw[i].hi;
+                pa.w_lo[i] = pw[i].lo;
+                pa.ldw[i] = pw[i].ld_split;
+                pa.M[i] = M[i];
+                pa.K[i] = K[i];
+                pa.kchunk[i] = tf32_chunk_blocks(K[i]);
+            }
+            PanelChain pc;
+            cudaError_t e = panel_chain_desc(pa, pc);
+            if (e != cudaSuccess)
+                return fail(FG_ERR_INVALID, "chain %d: panel tables: %s", j, cudaGetErrorString(e));
+            gx.panel.push_back(pc);
+            for (int i = 0; i < n; ++i) gx.panel_flops += gemm_flops(M[i], N, K[i]);
+            continue;
+        }
         if (dtype == FG_DT_F32) {  // 3xTF32 on the registered hi / lo split
             float *xh = (float *)cv.take((size_t)K[0] * ldN * 4);
             float *xl = (float *)cv.take((size_t)K[0] * ldN * 4);
@@ -348,7 +405,8 @@ int group_build(DevCtx *c, int dtype, int algo, int kernel, int order, int nchai
         }
         return FG_OK;
     }
-    const int nlaunch = order == FG_ORDER_LEVELS ? maxd + 1 : 1;
+    if (int st = panel_finish(c, gx, max_units)) return st;
+    const int nlaunch = all.empty() ? 0 : order == FG_ORDER_LEVELS ? maxd + 1 : 1;
     for (int lv = 0; lv < nlaunch; ++lv) {
         std::vector<StageArgs> st;
         std::vector<int> pv;
@@ -384,6 +442,9 @@ size_t group_tab_bytes(const GroupExec &gx)
     b += carve_size(done * sizeof(int) + 16);
     b += carve_size(gx.splits.size() * sizeof(SplitJob));
     for (auto &lv : gx.levels) b += carve_size(lv.jobs.size() * sizeof(FfmaJob));
+    b += carve_size(gx.panel.size() * sizeof(PanelChain)) +
+         carve_size(gx.panel_blocks.size() * sizeof(uint32_t)) +
+         carve_size(gx.panel_off.size() * sizeof(int));
     return b;
 }
 
@@ -402,6 +463,11 @@ void group_place(GroupExec &gx, Carver &cv)
     gx.splits_dev = gx.splits.empty() ? nullptr
                                       : (SplitJob *)cv.take(gx.splits.size() * sizeof(SplitJob));
     for (auto &lv : gx.levels) lv.dev = (FfmaJob *)cv.take(lv.jobs.size() * sizeof(FfmaJob));
+    if (!gx.panel.empty()) {
+        gx.panel_dev = (PanelChain *)cv.take(gx.panel.size() * sizeof(PanelChain));
+        gx.panel_blocks_dev = (uint32_t *)cv.take(gx.panel_blocks.size() * sizeof(uint32_t));
+        gx.panel_off_dev = (int *)cv.take(gx.panel_off.size() * sizeof(int));
+    }
 }
 
 int group_upload(const GroupExec &gx, cudaStream_t s, bool sync)
@@ -415,6 +481,12 @@ int group_upload(const GroupExec &gx, cudaStream_t s, bool sync)
         CUDA_TRY(copy(gx.tables[i], gx.gls[i].tables.data(), gx.gls[i].tables.size()));
     CUDA_TRY(copy(gx.splits_dev, gx.splits.data(), gx.splits.size() * sizeof(SplitJob)));
     for (auto &lv : gx.levels) CUDA_TRY(copy(lv.dev, lv.jobs.data(), lv.jobs.size() * sizeof(FfmaJob)));
+    if (!gx.panel.empty()) {
+        CUDA_TRY(copy(gx.panel_dev, gx.panel.data(), gx.panel.size() * sizeof(PanelChain)));
+        CUDA_TRY(copy(gx.panel_blocks_dev, gx.panel_blocks.data(),
+                      gx.panel_blocks.size() * sizeof(uint32_t)));
+        CUDA_TRY(copy(gx.panel_off_dev, gx.panel_off.data(), gx.panel_off.size() * sizeof(int)));
+    }
     return FG_OK;
 }
 
@@ -422,6 +494,14 @@ int group_launch(DevCtx *c, const GroupExec &gx, cudaStream_t s, bool capturing,
                  int *status)
 {
     if (!status) status = c->status;
+    if (!gx.panel.empty()) {
+        int st = run_kernel_on(c, s, capturing, FG_PK_TC_TF32X3, gx.panel_flops,
+                               "panel-resident chains", [&] {
+            return launch_panel(gx.panel_dev, gx.panel_blocks_dev, gx.panel_off_dev, gx.panel_ctas,
+                                status, s);
+        });
+        if (st) return st;
+    }
     if (gx.done_ints) CUDA_TRY(cudaMemsetAsync(gx.done, 0, gx.done_ints * sizeof(int), s));
     if (!gx.splits.empty()) {
         int st = run_kernel_on(c, s, capturing, FG_PK_AUX, 0.0, "tf32 split (group)", [&] {

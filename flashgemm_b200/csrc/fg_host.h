@@ -244,11 +244,27 @@ struct GroupExec {
         double flops = 0.0;
     };
     std::vector<Level> levels;         // plain FP32: one grouped launch per depth
+    // 3xTF32 chains small enough to run panel-resident (fg_panel.cu): one launch
+    std::vector<PanelChain> panel;
+    std::vector<uint32_t> panel_blocks;
+    std::vector<int> panel_off;
+    int panel_ctas = 0;
+    double panel_flops = 0.0;
+    PanelChain *panel_dev = nullptr;
+    uint32_t *panel_blocks_dev = nullptr;
+    int *panel_off_dev = nullptr;
     int kernels() const
     {
-        return (int)gls.size() + (splits.empty() ? 0 : 1) + (int)levels.size();
+        return (int)gls.size() + (splits.empty() ? 0 : 1) + (int)levels.size() +
+               (panel.empty() ? 0 : 1);
     }
 };
+
+// FP32 3xTF32 chains with every dimension at most kPanelKMax run panel-resident
+// (FG_PANEL=0: never).
+bool panel_enabled();
+// Plan the panel launch of gx.panel (blocks to CTAs; at most max_units CTAs, 0: all SMs).
+int panel_finish(DevCtx *c, GroupExec &gx, int max_units = 0);
 
 extern std::atomic<int> g_group_kernel, g_group_order;  // fg_set_group_config
 

@@ -3,6 +3,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -57,6 +58,11 @@ cudaError_t launch_tc_stage(const StageArgs &a, int num_sms, cudaStream_t s);
 cudaError_t launch_tc_chain(const StageArgs *stages, int n, int *done, int *status,
                             unsigned long long *trace, int num_sms, cudaStream_t s);
 int chain_max_stages();
+// Time-out self-test (fg_selftest_timeout): two BF16 stages whose second waits
+// on counters nothing releases; waits limited to limit_ns for this launch only.
+// `done`: 3 * chain_counter_ints(2, ...) zeroed ints.
+cudaError_t launch_tc_chain_stuck(const StageArgs *stages, int *done, int *status, int num_sms,
+                                  unsigned long long limit_ns, cudaStream_t s);
 // Counters a fused chain of these row counts (n stages, N columns) may use.
 size_t chain_counter_ints(int n, const long *M, long N);
 int chain_trace_fields();
@@ -96,20 +102,29 @@ struct SchedStage {
 // makespan (optional): the estimated finish time of the last tile.
 // starts (optional): each entry's estimated start, in the order of `entries`.
 //
-// Feeders (optional): the last `workers` workers take the last `rows` row tiles
-// of every column block of stage `stage` (row tile by row tile, after that
-// stage's other tiles, which they do not take) and no tile of the stage that
-// reads it. The readers, streamed, start on a column block while the feeders
-// still produce its last rows, instead of all waiting for the whole stage.
-// Every worker's list stays in stage order, so no worker waits forever.
-struct Feeders {
-    int stage = -1;  // -1: none
-    int workers = 0;
-    int rows = 0;
+// Options (optional argument):
+// * feeders: the last `feed_workers` workers take the last `feed_rows` row
+//   tiles of every column block of stage `feed_stage` (row tile by row tile,
+//   after that stage's other tiles, which they do not take) and no tile of the
+//   stage that reads it. The readers, streamed, start on a column block while
+//   the feeders still produce its last rows, instead of all waiting for the
+//   whole stage.
+// * window: the tiles are placed `window` column blocks at a time, every stage
+//   of those blocks before the next blocks' (0: each stage whole, in order), so
+//   that an intermediate is read back soon after it is written (stages that
+//   share the column blocks: one chain).
+// The placement order is a topological order of the tiles (a tile's inputs
+// come earlier), and every worker runs its tiles in that order, so no worker
+// waits forever.
+struct SchedOpts {
+    int feed_stage = -1;  // -1: no feeders
+    int feed_workers = 0;
+    int feed_rows = 0;
+    int window = 0;
 };
 void list_schedule(const SchedStage *st, int n, int units, double handoff, std::vector<int> &off,
                    std::vector<WorkEntry> &entries, double *makespan = nullptr,
-                   std::vector<double> *starts = nullptr, const Feeders *feed = nullptr);
+                   std::vector<double> *starts = nullptr, const SchedOpts *opts = nullptr);
 
 enum GroupKernel : int {
     GK_PAIR = 0,        // BF16 / INT8: CTA pairs, 256 x 256 tiles, 6-stage ring
@@ -148,6 +163,58 @@ cudaError_t plan_single_group(const StageArgs *stages, const int *prev, int n, i
                               int num_sms, GroupLaunch &out);
 cudaError_t launch_single_group(const GroupLaunch &g, const void *tables_dev, int *done,
                                 int *status, cudaStream_t s);
+
+// ------------------------------------------------------------------ panel-resident chains
+//
+// FP32 (3xTF32) chains whose every dimension (K_1 and every M_i) is at most
+// kPanelKMax run with their intermediates in shared memory (fg_panel.cu): one
+// CTA per 128-column block, B read once, only the last stage's result written.
+
+constexpr int kPanelKMax = 64;
+constexpr int kPanelMaxStages = 8;
+
+// One chain's device descriptor (tensor maps and shapes).
+struct alignas(64) PanelChain {
+    CUtensorMap tm_b;                        // B: K[0] x N FP32, MN-major boxes
+    CUtensorMap tm_c;                        // C: M_last x N FP32 (staged TMA stores)
+    CUtensorMap tm_w[kPanelMaxStages][2];    // weights (hi, lo), K-major boxes of 128 rows
+    int n;                                   // stages
+    int N;
+    int K[kPanelMaxStages + 1];              // K[i]: stage i's depth; K[i + 1] = M_i
+    int kchunk[kPanelMaxStages];             // k-blocks per FP32 promotion of the partial sum
+};
+
+// One launch: every CTA runs blocks[off[cta] .. off[cta + 1]) (chain << 16 | block).
+struct PanelArgs {
+    const PanelChain *chains;
+    const uint32_t *blocks;
+    const int *off;
+    int *status;
+};
+
+// Host description of one chain for panel_chain_desc (device pointers).
+struct PanelChainArgs {
+    int n;
+    long N;
+    const float *B;
+    long ldb;
+    float *C;
+    long ldc;
+    const float *w_hi[kPanelMaxStages], *w_lo[kPanelMaxStages];
+    long ldw[kPanelMaxStages];
+    long M[kPanelMaxStages], K[kPanelMaxStages];
+    int kchunk[kPanelMaxStages];
+};
+
+bool panel_eligible(long N, int n, const long *M, const long *K);
+cudaError_t panel_chain_desc(const PanelChainArgs &a, PanelChain &out);
+int panel_blocks_of(long N);
+// Blocks of the chains (stage_kb[c]: chain c's k-blocks per block, a cost) to `ctas` CTAs.
+void panel_plan(const std::vector<int> &stage_kb, const std::vector<int> &nblocks, int ctas,
+                std::vector<uint32_t> &blocks, std::vector<int> &off);
+cudaError_t panel_capacity(int num_sms, int &ctas);
+cudaError_t launch_panel(const PanelChain *chains_dev, const uint32_t *blocks_dev, const int *off_dev,
+                         int ctas, int *status, cudaStream_t s);
 
 // Plain FP32 SGEMM on CUDA cores: C = A * B, one FMA per k in increasing k;
 // with kblock > 0 each block of kblock k is summed from zero and added to C.

@@ -24,6 +24,16 @@ enum : int {
 
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s: far above any legal wait
 
+// The limit every bounded wait of a kernel compiled in this translation unit
+// uses: kWaitLimitNs, except where the host lowers it (stream-ordered, around
+// one launch) to make a wait run out on purpose (the time-out self-test).
+static __device__ unsigned long long fg_wait_limit_ns = kWaitLimitNs;
+
+__device__ __forceinline__ uint64_t wait_limit_ns()
+{
+    return *reinterpret_cast<volatile unsigned long long *>(&fg_wait_limit_ns);
+}
+
 __device__ __forceinline__ uint64_t globaltimer_ns()
 {
     uint64_t t;
@@ -85,9 +95,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *s
     const uint32_t a = smem_u32(bar);
     if (mbar_try_wait(a, parity)) return true;
     const uint64_t t0 = globaltimer_ns();
+    const uint64_t limit = wait_limit_ns();
     while (true) {
         if (mbar_try_wait(a, parity)) return true;
-        if (globaltimer_ns() - t0 > kWaitLimitNs) {
+        if (globaltimer_ns() - t0 > limit) {
             atomicCAS(status, 0, code);
             return false;
         }

@@ -58,7 +58,8 @@ struct fg_server_s {
     std::vector<int> free_slots;
     std::unordered_map<long long, Req *> reqs;
     size_t used = 0, peak = 0;
-    long long next_id = 0, submitted = 0, completed = 0, failed = 0, batches = 0, batched = 0;
+    long long next_id = 0, submitted = 0, completed = 0, failed = 0, shed = 0, batches = 0,
+              batched = 0;
     std::vector<double> lat;
     double flops = 0.0, t_first = -1.0, t_last = 0.0;
     bool stop = false;
@@ -203,8 +204,30 @@ void server_dispatch_loop(fg_server_s *s)
     std::unique_lock<std::mutex> lk(s->mu);
     while (true) {
         if (s->stop && s->pending.empty()) break;
+        if (s->o.max_queue_us > 0) {
+            // load shedding: requests queued past their deadline are not run
+            const double t = now_us();
+            bool any = false;
+            while (!s->pending.empty() && t - s->pending.front()->t_submit > s->o.max_queue_us) {
+                fg_server_s::Req *q = s->pending.front();
+                s->pending.pop_front();
+                q->done = true;
+                q->status = FG_ERR_BUSY;
+                q->latency_us = t - q->t_submit;
+                ++s->shed;
+                any = true;
+            }
+            if (any) s->cv_done.notify_all();
+        }
         if (s->pending.empty() || s->free_slots.empty()) {
-            s->cv_dispatch.wait_for(lk, std::chrono::milliseconds(5));
+            // a slot frees when a batch completes; with shedding on, wake in time
+            // to shed the oldest request at its deadline
+            long wait_us = 5000;
+            if (s->o.max_queue_us > 0 && !s->pending.empty()) {
+                const double left = s->o.max_queue_us - (now_us() - s->pending.front()->t_submit);
+                wait_us = std::max(1l, std::min(wait_us, (long)left + 1));
+            }
+            s->cv_dispatch.wait_for(lk, std::chrono::microseconds(wait_us));
             continue;
         }
         // busy device: wait for a full batch or the oldest request's window
@@ -419,7 +442,7 @@ FG_EXPORT int fg_server_drain(fg_server s)
 {
     if (!s) return fail(FG_ERR_INVALID, "null server");
     std::unique_lock<std::mutex> lk(s->mu);
-    while (s->completed + s->failed < s->submitted) s->cv_done.wait(lk);
+    while (s->completed + s->failed + s->shed < s->submitted) s->cv_done.wait(lk);
     return ok();
 }
 
@@ -431,6 +454,7 @@ FG_EXPORT int fg_server_get_stats(fg_server s, fg_server_stats *out)
     out->submitted = s->submitted;
     out->completed = s->completed;
     out->failed = s->failed;
+    out->shed = s->shed;
     out->batches = s->batches;
     out->mean_batch = s->batches ? (double)s->batched / (double)s->batches : 0.0;
     std::vector<double> v = s->lat;
@@ -460,8 +484,8 @@ FG_EXPORT int fg_server_reset_stats(fg_server s)
     if (!s) return fail(FG_ERR_INVALID, "null server");
     std::lock_guard<std::mutex> lk(s->mu);
     s->lat.clear();
-    s->submitted -= s->completed + s->failed;
-    s->completed = s->failed = 0;
+    s->submitted -= s->completed + s->failed + s->shed;
+    s->completed = s->failed = s->shed = 0;
     s->batches = s->batched = 0;
     s->flops = 0.0;
     s->t_first = -1.0;

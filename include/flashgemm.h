@@ -29,10 +29,13 @@
 extern "C" {
 #endif
 
-/* Thread count the reference's OpenMP team uses (flashgemm.c:6). Here it only
- * decides where the reference's 32-column panels start (strip width
- * 16 * ceil(ceil(N / 16) / T), flashgemm.c:40-52); the GPU uses no host
- * threads. Replaces flashgemm.h:17. */
+/* Thread count the reference's OpenMP team uses (flashgemm.c:6). Here it is
+ * stored and read back, and changes no result: the GPU uses no host threads,
+ * and the reference's 32-column panels always start at multiples of 32
+ * columns, which is where the reference's strips put them whenever its strip
+ * width 16 * ceil(ceil(N / 16) / T) is a multiple of 32 (flashgemm.c:40-52),
+ * i.e. on every input whose result the reference defines. Replaces
+ * flashgemm.h:17. */
 extern int flashgemm_thread_num;
 
 /* Replaces flashgemm.h:19 / flashgemm.c:8-11. */

@@ -24,7 +24,8 @@ typedef enum {
     FG_ERR_CUDA = 3,        /* a CUDA runtime call failed */
     FG_ERR_NO_DEVICE = 4,   /* no usable sm_100 device */
     FG_ERR_TIMEOUT = 5,     /* a kernel's bounded pipeline wait ran out */
-    FG_ERR_NOMEM = 6        /* device scratch allocation failed */
+    FG_ERR_NOMEM = 6,       /* device scratch allocation failed */
+    FG_ERR_BUSY = 7         /* serving: the request was shed (queued past max_queue_us) */
 } fg_status;
 
 /* Status and message of the last call made on this host thread. */
@@ -205,6 +206,10 @@ typedef struct {
     int slots;             /* batches in flight at once (0: 2) */
     int max_wait_us;       /* batching window while the device is busy (0: 200) */
     int ctas_per_batch;    /* grid cap of a batch's grouped kernels (0: SMs / slots) */
+    int max_queue_us;      /* load shedding: a request still queued (not yet admitted)
+                              this long after its submit is completed with FG_ERR_BUSY
+                              instead of run, so that under overload the latency of the
+                              requests that are served stays bounded (0: never shed) */
 } fg_server_opts;
 
 typedef struct {
@@ -221,6 +226,7 @@ typedef struct {
 
 typedef struct {
     long long submitted, completed, failed;
+    long long shed;         /* requests completed with FG_ERR_BUSY (max_queue_us) */
     long long batches;      /* batches launched */
     double mean_batch;      /* requests per batch */
     double p50_us, p99_us, mean_us, max_us;  /* latency, submit to completion */
@@ -256,6 +262,17 @@ int fg_server_destroy(fg_server s);
  * time-out of a fg_chain_bf16_noalloc call made with status == NULL, once the
  * caller's stream has finished that call. */
 int fg_sync(void);
+
+/* Self-test of failure detection; no counterpart in the reference (whose
+ * only error path is print-and-return). Runs a small fused BF16 chain in which
+ * the second stage waits on a dependency that nothing releases, with every
+ * bounded wait of that one launch limited to limit_us microseconds (100 ..
+ * 1000000). The waits run out, the kernel records the cause in the device
+ * status word, stops its pipelines, frees its tensor memory and returns; this
+ * call then returns what the host read: FG_ERR_TIMEOUT (message in
+ * fg_last_error) when detection works. Nothing faults or hangs, and later calls
+ * on the device run normally (the limit is restored in stream order). */
+int fg_selftest_timeout(int limit_us);
 
 /* Number of kernels this library has launched in this process (all devices).
  * Lets a benchmark count its own launches. */

@@ -39,8 +39,32 @@ def _weight_sets(fg, seed):
         K1 = int(rng.choice([64, 128, 256, 512]))
         Ms = [int(rng.choice([64, 96, 200, 256, 520])) for _ in range(n)]
         _, As, Ks = oracle.chain_inputs(dt, 64, K1, Ms, seed=seed + j)
-        sets.append((dt, K1, Ms, [fg.Weights(dt, a) for a in As]))
+        sets.append((dt, K1, Ms, [fg.Weights(dt, a) for a in As], As))
     return sets
+
+
+def _release(sets):
+    for st in sets:
+        for w in st[3]:
+            w.release()
+
+
+def _oracle_check(fg, dt, As, B, got, N, Ms):
+    """The request's result against the oracle: INT8 bit-exact (written rows),
+    BF16 within the parity tolerance of the reference semantics, FP32 (3xTF32)
+    within 2x the plain FP32 kernel's own error against FP64."""
+    Ks = [As[0].shape[1]] + list(Ms[:-1])
+    if dt == "int8":
+        want = oracle.chain(dt, B.view(np.uint8), As, N, Ms, Ks, mode=oracle.REF, threads=1)
+        rows = (Ms[-1] // 4) * 4
+        np.testing.assert_array_equal(got[:rows], want[:rows])
+    elif dt == "bf16":
+        want = oracle.chain(dt, B, As, N, Ms, Ks, mode=oracle.REF, threads=1)
+        assert oracle.rel_frob(got, want) <= 2e-3
+    else:
+        exact = oracle.chain_f64(B, As, N, Ms, Ks)
+        plain = oracle.chain("f32", B, As, N, Ms, Ks)
+        assert oracle.rel_frob(got, exact) <= 2 * oracle.rel_frob(plain, exact)
 
 
 def _inputs(dt, K1, N, seed):
@@ -83,7 +107,7 @@ def test_results_same_alone_and_in_the_mix(fg):
     def client(k):
         rnd = random.Random(k)
         for i in range(24):
-            dt, K1, Ms, W = sets[rnd.randrange(len(sets))]
+            dt, K1, Ms, W, As = sets[rnd.randrange(len(sets))]
             N = rnd.choice([16, 64, 128, 272, 512])
             B = _inputs(dt, K1, N, 1000 * k + i)
             odt = np.int32 if dt == "int8" else np.float32
@@ -97,7 +121,7 @@ def test_results_same_alone_and_in_the_mix(fg):
                 C = np.full((Ms[-1], N), 9, odt)
                 rid = srv.submit(dt, W, B, C)
             with lock:
-                reqs.append((rid, dt, W, B, C, N, Ms[-1]))
+                reqs.append((rid, dt, W, B, C, N, Ms, As))
             time.sleep(rnd.expovariate(4000.0))
 
     th = [threading.Thread(target=client, args=(k,)) for k in range(2)]
@@ -110,13 +134,13 @@ def test_results_same_alone_and_in_the_mix(fg):
     assert st["completed"] == len(reqs) and st["failed"] == 0
     assert st["batches"] < len(reqs)  # arrivals were batched
     assert st["p99_us"] >= st["p50_us"] > 0 and all(x > 0 for x in lats)
-    for rid, dt, W, B, C, N, Ml in reqs:
+    for k, (rid, dt, W, B, C, N, Ms, As) in enumerate(reqs):
         got = C.cpu().numpy() if not isinstance(C, np.ndarray) else C
-        _same(dt, got, _alone(fg, dt, W, B, N, Ml), Ml)
+        _same(dt, got, _alone(fg, dt, W, B, N, Ms[-1]), Ms[-1])
+        if k % 4 == 0:  # a sample of the mix, against the oracle directly
+            _oracle_check(fg, dt, As, B, got, N, Ms)
     srv.close()
-    for *_, W in sets:
-        for w in W:
-            w.release()
+    _release(sets)
 
 
 def test_admission_by_device_memory(fg):
@@ -124,7 +148,7 @@ def test_admission_by_device_memory(fg):
     (admitted as memory frees up), the held bytes never exceed the budget, and
     a request larger than the whole budget fails alone without stalling the rest."""
     sets = _weight_sets(fg, 80)
-    dt, K1, Ms, W = sets[0]
+    dt, K1, Ms, W, _ = sets[0]
     N = 256
     budget = 3 << 20
     srv = fg.Server(hbm_budget=budget, max_batch=16, slots=2)
@@ -148,14 +172,12 @@ def test_admission_by_device_memory(fg):
     for B, C in outs:
         _same(dt, C, _alone(fg, dt, W, B, N, Ms[-1]), Ms[-1])
     srv.close()
-    for *_, Wx in sets:
-        for w in Wx:
-            w.release()
+    _release(sets)
 
 
 def test_burst_is_batched_and_stats_reset(fg):
     sets = _weight_sets(fg, 90)
-    dt, K1, Ms, W = sets[1]
+    dt, K1, Ms, W, _ = sets[1]
     srv = fg.Server(max_batch=32, slots=2)
     B = _inputs(dt, K1, 128, 4000)
     Cs = [np.zeros((Ms[-1], 128), np.int32) for _ in range(96)]
@@ -173,6 +195,35 @@ def test_burst_is_batched_and_stats_reset(fg):
     st = srv.stats()
     assert st["completed"] == 0 and st["batches"] == 0
     srv.close()
-    for *_, Wx in sets:
-        for w in Wx:
-            w.release()
+    _release(sets)
+
+
+def test_load_shedding_bounds_queueing(fg):
+    """A burst far above what the loop can admit within max_queue_us: the
+    requests still queued at their deadline are shed (FG_ERR_BUSY, outputs
+    untouched), every other request completes with the right result, and the
+    counts add up."""
+    sets = _weight_sets(fg, 95)
+    dt, K1, Ms, W, As = sets[0]
+    N = 512
+    srv = fg.Server(max_batch=4, slots=1, max_queue_us=300)
+    B = _inputs(dt, K1, N, 5000)
+    Cs = [np.full((Ms[-1], N), 7.0, np.float32) for _ in range(200)]
+    ids = [srv.submit(dt, W, B, C) for C in Cs]
+    srv.drain()
+    st = srv.stats()
+    assert st["shed"] > 0 and st["completed"] > 0 and st["failed"] == 0
+    assert st["completed"] + st["shed"] == 200
+    want = _alone(fg, dt, W, B, N, Ms[-1])
+    served = 0
+    for rid, C in zip(ids, Cs):
+        lat = srv.wait(rid, shed_ok=True)
+        if lat is None:
+            assert (C == 7.0).all()  # never run
+            continue
+        served += 1
+        _same(dt, C, want, Ms[-1])
+    assert served == st["completed"]
+    _oracle_check(fg, dt, As, B, want, N, Ms)
+    srv.close()
+    _release(sets)
