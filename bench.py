@@ -1012,13 +1012,22 @@ def run_chain_bench(args, g, workload, peaks_run=None):
     reference's CPU time. Returns the line on rank 0, else None."""
     torch, fg, dist, dev = g.torch, g.fg, g.dist, g.dev
     world, rank = g.world, g.rank
-    dt, N, K1, Ms = WORKLOADS[workload]
+    dt, N_all, K1, Ms = WORKLOADS[workload]
+    strong = args.scaling == "strong" and world > 1 and dt != "f32"
+    if strong:
+        # the ranks split one chain's columns (fg_split_columns), no collective
+        c0, c1 = fg.shard_columns(N_all, world, rank)
+        N = c1 - c0
+    else:
+        N = N_all
     metric = {"f32": "FP32 GEMM TFLOP/s"}.get(dt, "fused GEMM-chain TFLOP/s")
-    config = {"workload": DESCR[workload], "dtype": dt, "N": N, "K1": K1, "M": Ms,
+    config = {"workload": DESCR[workload], "dtype": dt, "N": N_all, "K1": K1, "M": Ms,
               "gflop_per_step_per_gpu": flops_of(N, K1, Ms) / 1e9,
               "semantics": "reference (panel permutation, INT8 tail rows)",
               "l2": "flushed between steps (256 MiB write outside the step events)",
-              "parallelism": f"dp{world} (activation columns partitioned, no collective)"}
+              "parallelism": (f"dp{world} (one chain's {N_all} columns split across the ranks on "
+                              "32-column panel boundaries, no collective)" if strong else
+                              f"dp{world} (activation columns partitioned, no collective)")}
 
     # --------------------------------------------------------- device-resident step
     B, As, Ks = make_inputs(dt, N, K1, Ms, seed=1234 + rank)
@@ -1131,8 +1140,11 @@ def run_chain_bench(args, g, workload, peaks_run=None):
     total_ms, = g.max_over_ranks(total_ms)
     if per_gemm:
         per_gemm = (g.max_over_ranks(per_gemm[0])[0], per_gemm[1])
+    cublas, = g.max_over_ranks(cublas)
     step_flops = flops_of(N, K1, Ms)
-    value = world * step_flops * args.steps / (total_ms / 1e3) / 1e12
+    # whole-job work per step: every rank's columns (weak: N each; strong: one chain)
+    job_flops = flops_of(N_all, K1, Ms) if strong else world * step_flops
+    value = job_flops * args.steps / (total_ms / 1e3) / 1e12
 
     # --------------------------------------------------------- end to end through the C ABI
     e2e_steps = args.e2e_steps or min(args.steps, 200)
@@ -1158,7 +1170,7 @@ def run_chain_bench(args, g, workload, peaks_run=None):
         for _ in range(e2e_steps):
             one()
         sec, = g.max_over_ranks(time.perf_counter() - t0)
-        return world * step_flops * e2e_steps / sec / 1e12
+        return job_flops * e2e_steps / sec / 1e12
 
     pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
     out_np = np.int32 if dt == "int8" else np.float32
@@ -1213,7 +1225,8 @@ def run_chain_bench(args, g, workload, peaks_run=None):
 
     line = {"metric": metric, "value": value, "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dt,
+            "higher_is_better": True, "scaling": "strong" if strong else "weak",
+            "vs_baseline": None, "dtype": dt,
             "data": "synthetic (seeded; no dataset involved)", "config": config,
             "clocks": sampler.summary(), "gpu_launches": launches,
             "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
@@ -1223,13 +1236,13 @@ def run_chain_bench(args, g, workload, peaks_run=None):
                     "pageable_api": "the same calls on ordinary (pageable) host buffers"},
             "roofline": roofline, "wall_s_timed_region": t_wall}
     if per_gemm:
-        pg_value = world * step_flops * args.steps / (per_gemm[0] / 1e3) / 1e12
+        pg_value = job_flops * args.steps / (per_gemm[0] / 1e3) / 1e12
         line["per_gemm"] = {"value": pg_value, "unit": "TFLOP/s",
                             "ms_per_step": per_gemm[0] / args.steps,
                             "launches": per_gemm[1],
                             "path": "one tensor-core launch per GEMM (FG_CHAIN_PER_GEMM)"}
         line["fused_vs_per_gemm"] = value / pg_value
-    cb_value = world * step_flops * args.steps / (cublas / 1e3) / 1e12
+    cb_value = job_flops * args.steps / (cublas / 1e3) / 1e12
     if dt == "f32":
         line["cublas_sgemm"] = {"value": cb_value, "unit": "TFLOP/s",
                                 "ms_per_step": cublas / args.steps,
@@ -1295,6 +1308,9 @@ def main():
     ap.add_argument("--serve-rates", type=float, nargs="+", default=None,
                     help="serve: offered rates as fractions of the measured capacity "
                          "(default 0.3 0.6 0.9; 0.6 within 'all')")
+    ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                    help="N > 1, chain workloads: weak (every rank its own full chain) or "
+                         "strong (the ranks split one chain's columns)")
     ap.add_argument("--serve-deadline-us", type=int, default=20000,
                     help="serve: the server sheds requests still queued this long after submit")
     ap.add_argument("--e2e-steps", type=int, default=None,

@@ -256,20 +256,44 @@ def profile_query(kind=-1):
 
 # ------------------------------------------------------------ multi-GPU partitioning
 
-def shard_columns(N, world, rank, panel=32):
+def shard_columns(N, world, rank):
     """Column range [start, stop) of the activations/outputs that `rank` of
-    `world` owns when one chain is split across GPUs. The chain is independent
-    per column except that the reference's between-stage permutation mixes the
-    columns of each 32-column panel, so shards are cut on panel boundaries:
-    each rank then runs the unchanged chain on its slice of B and writes its
-    slice of C, with no collective on the data path."""
+    `world` owns when one chain is split across GPUs (the library's
+    fg_split_columns; host arithmetic, no device needed). The chain is
+    independent per column except that the reference's between-stage
+    permutation mixes the columns of each 32-column panel, so shards are cut on
+    panel boundaries: each rank then runs the unchanged chain on its slice of B
+    and writes its slice of C, with no collective on the data path."""
     if world < 1 or not 0 <= rank < world:
         raise ValueError("bad world/rank")
-    panels = (N + panel - 1) // panel
-    per, extra = divmod(panels, world)
-    p0 = rank * per + min(rank, extra)
-    p1 = p0 + per + (1 if rank < extra else 0)
-    return min(p0 * panel, N), min(p1 * panel, N)
+    L = lib()
+    L.fg_split_columns.argtypes = [_L, ctypes.c_int, ctypes.c_int, _P, _P]
+    c0, c1 = ctypes.c_long(), ctypes.c_long()
+    st = L.fg_split_columns(int(N), int(world), int(rank), ctypes.byref(c0), ctypes.byref(c1))
+    if st != FG_OK:
+        raise FlashgemmError(st, last_error())
+    return c0.value, c1.value
+
+
+def chain_multi_device(dtype, C, B, N, As, Ms, Ks, devices):
+    """One chain on host (numpy) operands split by columns across `devices`
+    (fg_chain_multi_device): the reference entry points' semantics, bit for
+    bit the single-device result."""
+    L = lib()
+    L.fg_chain_multi_device.argtypes = [ctypes.c_int, _P, _P, _L, ctypes.c_int, _P, _P, _P,
+                                        ctypes.c_int, _P]
+    n = len(As)
+    adt = {"f32": np.float32, "bf16": np.uint16, "int8": np.int8}[dtype]
+    bdt = {"f32": np.float32, "bf16": np.uint16, "int8": np.uint8}[dtype]
+    odt = np.int32 if dtype == "int8" else np.float32
+    aptr = (_P * n)(*[_host_ptr(a, adt) for a in As])
+    ms = (ctypes.c_long * n)(*[int(m) for m in Ms])
+    ks = (ctypes.c_long * n)(*[int(k) for k in Ks])
+    dv = (ctypes.c_int * len(devices))(*[int(d) for d in devices])
+    st = L.fg_chain_multi_device(_DT[dtype], _host_ptr(C, odt), _host_ptr(B, bdt), int(N), n, aptr,
+                                 ms, ks, len(devices), dv)
+    if st != FG_OK:
+        raise FlashgemmError(st, last_error())
 
 
 # ------------------------------------------------------------ weight registry

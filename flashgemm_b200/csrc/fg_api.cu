@@ -151,6 +151,7 @@ int get_ctx(DevCtx **out)
         for (int j = 0; j < DevCtx::kCopyChunks; ++j) {
             CUDA_TRY(cudaEventCreateWithFlags(&c->ev_up[j], cudaEventDisableTiming));
             CUDA_TRY(cudaEventCreateWithFlags(&c->ev_done[j], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&c->ev_down[j], cudaEventDisableTiming));
         }
         CUDA_TRY(cudaMalloc(&c->status, sizeof(int)));
         CUDA_TRY(cudaMemset(c->status, 0, sizeof(int)));
@@ -709,9 +710,129 @@ cudaError_t copy_rows(void *dst, size_t dpitch, const void *src, size_t spitch, 
     return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, kind, s);
 }
 
+// ---------------------------------------------------------------- host copies
+
+RowCopier::RowCopier(int threads) : parts_(threads < 1 ? 1 : threads)
+{
+    for (int i = 1; i < parts_; ++i) th_.emplace_back([this, i] { run(i); });
+}
+
+RowCopier::~RowCopier()
+{
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        stop_ = true;
+    }
+    cv_go_.notify_all();
+    for (auto &t : th_) t.join();
+}
+
+namespace {
+void copy_part(char *dst, size_t dpitch, const char *src, size_t spitch, size_t width, size_t r0,
+               size_t r1)
+{
+    if (r1 <= r0) return;
+    if (dpitch == width && spitch == width) {
+        memcpy(dst + r0 * width, src + r0 * width, (r1 - r0) * width);
+        return;
+    }
+    for (size_t r = r0; r < r1; ++r) memcpy(dst + r * dpitch, src + r * spitch, width);
+}
+}  // namespace
+
+void RowCopier::run(int part)
+{
+    unsigned long long seen = 0;
+    while (true) {
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_go_.wait(lk, [&] { return stop_ || gen_ != seen; });
+            if (stop_) return;
+            seen = gen_;
+        }
+        copy_part(dst_, dpitch_, src_, spitch_, width_, height_ * part / parts_,
+                  height_ * (part + 1) / parts_);
+        std::lock_guard<std::mutex> lk(mu_);
+        if (--pending_ == 0) cv_done_.notify_one();
+    }
+}
+
+void RowCopier::copy(void *dst, size_t dpitch, const void *src, size_t spitch, size_t width,
+                     size_t height)
+{
+    char *d = static_cast<char *>(dst);
+    const char *sp = static_cast<const char *>(src);
+    if (parts_ == 1 || height < (size_t)parts_ || width * height < (256u << 10)) {
+        copy_part(d, dpitch, sp, spitch, width, 0, height);
+        return;
+    }
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        dst_ = d;
+        src_ = sp;
+        dpitch_ = dpitch;
+        spitch_ = spitch;
+        width_ = width;
+        height_ = height;
+        pending_ = parts_ - 1;
+        ++gen_;
+    }
+    cv_go_.notify_all();
+    copy_part(d, dpitch, sp, spitch, width, 0, height / parts_);
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_done_.wait(lk, [&] { return pending_ == 0; });
+}
+
+// How a host operand reaches the device: page-locked memory (or managed) is
+// copied by DMA directly; ordinary pageable memory goes through pinned staging.
+enum class HostMem { Pinned, Pageable, Device };
+HostMem host_mem(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return HostMem::Pageable;
+    }
+    if (a.type == cudaMemoryTypeDevice) return HostMem::Device;
+    return a.type == cudaMemoryTypeUnregistered ? HostMem::Pageable : HostMem::Pinned;
+}
+
+int pin_reserve(DevCtx *c, size_t bytes)
+{
+    if (bytes <= c->pin_cap) return FG_OK;
+    if (c->pin) cudaFreeHost(c->pin);  // every earlier host-pointer call has completed
+    c->pin = nullptr;
+    c->pin_cap = 0;
+    const size_t cap = bytes + bytes / 4;
+    cudaError_t e = cudaMallocHost(&c->pin, cap);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(FG_ERR_NOMEM, "pinned staging of %zu bytes: %s", cap, cudaGetErrorString(e));
+    }
+    c->pin_cap = cap;
+    if (!c->copier) {
+        const unsigned hw = std::thread::hardware_concurrency();
+        c->copier.reset(new RowCopier((int)std::max(1u, std::min(8u, hw / 2))));
+    }
+    return FG_OK;
+}
+
 // Host-pointer chain: stage operands into device scratch, run, copy C back.
+// B and C rows are ldb and ldc elements apart (N for the reference's dense
+// operands; a column slice of a wider chain otherwise).
+//
+// Column chunks (fused BF16 / INT8 chains from 1024 columns): the weights and
+// then each chunk of B go up on one copy stream, each chunk's chain runs on the
+// compute stream once its columns are there, and its columns of C come back on
+// a second copy stream while later chunks compute. Chunks start on multiples
+// of 256 columns: every tile, panel and result is the one of the whole chain.
+// Operands in ordinary (pageable) host memory, which the reference's callers
+// pass (posix_memalign / malloc), pass through pinned staging: the copier's
+// threads move each piece while the copy engines move the previous one, the
+// weights in pieces of about 2 MB, B and C chunk by chunk, so that the overlap
+// survives; page-locked operands are copied directly.
 int host_chain(int dtype, void *C, const void *B, long N, int n, const void *const *A,
-               const long *M, const long *K)
+               const long *M, const long *K, long ldb, long ldc)
 {
     int st = check_shapes(dtype, N, n, M, K);
     if (st) return st;
@@ -738,6 +859,32 @@ int host_chain(int dtype, void *C, const void *B, long N, int n, const void *con
         need += carve_size((size_t)M[i] * lda[i] * elt);
     }
     need += chain_scratch(dtype, algo, N, n, M, K) + 4096;
+    // INT8 reference semantics leave rows >= 4 * floor(M / 4) of C untouched
+    // (multigemm/src/kernel_int8.h:943-945)
+    long rows = M[n - 1];
+    if (dtype == FG_DT_INT8 && sem == FG_SEM_REF) rows = (rows / 4) * 4;
+
+    // which operands need staging, and the pinned bytes they take
+    const HostMem mb = host_mem(B), mc = host_mem(C);
+    std::vector<HostMem> ma(n);
+    for (int i = 0; i < n; ++i) ma[i] = host_mem(A[i]);
+    bool dev_ptr = mb == HostMem::Device || mc == HostMem::Device;
+    for (int i = 0; i < n; ++i) dev_ptr = dev_ptr || ma[i] == HostMem::Device;
+    if (dev_ptr)
+        return fail(FG_ERR_INVALID, "host pointers expected (use fg_chain_dev for device memory)");
+    size_t pin_bytes = 0;
+    std::vector<size_t> pin_w(n, 0);
+    for (int i = 0; i < n; ++i)
+        if (ma[i] == HostMem::Pageable) {
+            pin_w[i] = pin_bytes;
+            pin_bytes += carve_size((size_t)M[i] * K[i] * elt);
+        }
+    const size_t pin_b = pin_bytes;
+    if (mb == HostMem::Pageable) pin_bytes += carve_size((size_t)K[0] * N * elt) + 256 * 4;
+    const size_t pin_c = pin_bytes;
+    if (mc == HostMem::Pageable) pin_bytes += carve_size((size_t)rows * N * out_elt) + 256 * 4;
+    if (pin_bytes && (st = pin_reserve(c, pin_bytes))) return st;
+
     if ((st = enter_stream(c, c->stream))) return st;
     if ((st = arena_reserve(c, need))) return st;
     // the uploads overwrite the arena: after every earlier call's kernels
@@ -752,16 +899,7 @@ int host_chain(int dtype, void *C, const void *B, long N, int n, const void *con
         ad[i] = Mat{wd[i], lda[i]};
     }
     void *cd = arena_take(c, (size_t)M[n - 1] * ldN * out_elt);
-    // INT8 reference semantics leave rows >= 4 * floor(M / 4) of C untouched
-    // (multigemm/src/kernel_int8.h:943-945)
-    long rows = M[n - 1];
-    if (dtype == FG_DT_INT8 && sem == FG_SEM_REF) rows = (rows / 4) * 4;
 
-    // Column chunks (fused BF16 / INT8 chains from 1024 columns): the weights and
-    // then each chunk of B go up on one copy stream, each chunk's chain runs on the
-    // compute stream once its columns are there, and its columns of C come back on
-    // a second copy stream while later chunks compute. Chunks start on multiples
-    // of 256 columns: every tile, panel and result is the one of the whole chain.
     const bool chunked = (dtype == FG_DT_BF16 || dtype == FG_DT_INT8) && fused_enabled() &&
                          N >= 1024;
     const int nchunk = chunked ? DevCtx::kCopyChunks : 1;
@@ -772,23 +910,47 @@ int host_chain(int dtype, void *C, const void *B, long N, int n, const void *con
         cudaStreamSynchronize(c->stream_d2h);
     };
     for (int i = 0; i < n; ++i) {
-        const cudaError_t e = copy_rows(wd[i], lda[i] * elt, A[i], K[i] * elt,
-                                                K[i] * elt, M[i], cudaMemcpyHostToDevice,
-                                                c->stream_h2d);
+        cudaError_t e = cudaSuccess;
+        const size_t row = (size_t)K[i] * elt;
+        if (ma[i] == HostMem::Pageable) {
+            // in pieces of about 2 MB: the next piece is staged while this one moves
+            char *pw = c->pin + pin_w[i];
+            const long piece = std::max(1l, (long)((2u << 20) / std::max<size_t>(row, 1)));
+            for (long r0 = 0; r0 < M[i] && e == cudaSuccess; r0 += piece) {
+                const long r1 = std::min(M[i], r0 + piece);
+                c->copier->copy(pw + r0 * row, row, static_cast<const char *>(A[i]) + r0 * row, row,
+                                row, r1 - r0);
+                e = copy_rows(static_cast<char *>(wd[i]) + r0 * lda[i] * elt, lda[i] * elt,
+                              pw + r0 * row, row, row, r1 - r0, cudaMemcpyHostToDevice,
+                              c->stream_h2d);
+            }
+        } else {
+            e = copy_rows(wd[i], lda[i] * elt, A[i], row, row, M[i], cudaMemcpyHostToDevice,
+                          c->stream_h2d);
+        }
         if (e != cudaSuccess) {
             drain();
             return fail(FG_ERR_CUDA, "chain upload: %s", cudaGetErrorString(e));
         }
     }
     const size_t mark = c->arena_off;
+    int chunks = 0;
     for (int j = 0; j < nchunk; ++j) {
         const long c0 = j * cw, c1 = c0 + cw < N ? c0 + cw : N;
         if (c0 >= N) break;
+        ++chunks;
+        const size_t wb = (size_t)(c1 - c0) * elt;
         char *bj = static_cast<char *>(bd) + c0 * elt;
         char *cj = static_cast<char *>(cd) + c0 * out_elt;
-        cudaError_t e = copy_rows(bj, ldN * elt, static_cast<const char *>(B) + c0 * elt,
-                                          N * elt, (c1 - c0) * elt, K[0], cudaMemcpyHostToDevice,
-                                          c->stream_h2d);
+        cudaError_t e;
+        if (mb == HostMem::Pageable) {
+            char *pb = c->pin + pin_b + (size_t)K[0] * c0 * elt;  // chunk j's columns, dense
+            c->copier->copy(pb, wb, static_cast<const char *>(B) + c0 * elt, ldb * elt, wb, K[0]);
+            e = copy_rows(bj, ldN * elt, pb, wb, wb, K[0], cudaMemcpyHostToDevice, c->stream_h2d);
+        } else {
+            e = copy_rows(bj, ldN * elt, static_cast<const char *>(B) + c0 * elt, ldb * elt, wb,
+                          K[0], cudaMemcpyHostToDevice, c->stream_h2d);
+        }
         if (e == cudaSuccess) e = cudaEventRecord(c->ev_up[j], c->stream_h2d);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_up[j], 0);
         if (e != cudaSuccess) {
@@ -803,13 +965,33 @@ int host_chain(int dtype, void *C, const void *B, long N, int n, const void *con
         }
         e = cudaEventRecord(c->ev_done[j], c->stream);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream_d2h, c->ev_done[j], 0);
-        if (e == cudaSuccess && rows > 0)
-            e = copy_rows(static_cast<char *>(C) + c0 * out_elt, N * out_elt, cj,
-                                  ldN * out_elt, (c1 - c0) * out_elt, rows,
-                                  cudaMemcpyDeviceToHost, c->stream_d2h);
+        const size_t wc = (size_t)(c1 - c0) * out_elt;
+        if (e == cudaSuccess && rows > 0) {
+            if (mc == HostMem::Pageable)
+                e = copy_rows(c->pin + pin_c + (size_t)rows * c0 * out_elt, wc, cj, ldN * out_elt,
+                              wc, rows, cudaMemcpyDeviceToHost, c->stream_d2h);
+            else
+                e = copy_rows(static_cast<char *>(C) + c0 * out_elt, ldc * out_elt, cj,
+                              ldN * out_elt, wc, rows, cudaMemcpyDeviceToHost, c->stream_d2h);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev_down[j], c->stream_d2h);
         if (e != cudaSuccess) {
             drain();
             return fail(FG_ERR_CUDA, "chain download: %s", cudaGetErrorString(e));
+        }
+    }
+    if (mc == HostMem::Pageable && rows > 0) {
+        // each chunk of C leaves staging as soon as it has arrived
+        for (int j = 0; j < chunks; ++j) {
+            const long c0 = j * cw, c1 = c0 + cw < N ? c0 + cw : N;
+            const cudaError_t e = cudaEventSynchronize(c->ev_down[j]);
+            if (e != cudaSuccess) {
+                drain();
+                return fail(FG_ERR_CUDA, "chain download: %s", cudaGetErrorString(e));
+            }
+            const size_t wc = (size_t)(c1 - c0) * out_elt;
+            c->copier->copy(static_cast<char *>(C) + c0 * out_elt, ldc * out_elt,
+                            c->pin + pin_c + (size_t)rows * c0 * out_elt, wc, wc, rows);
         }
     }
     CUDA_TRY(cudaStreamSynchronize(c->stream_d2h));
@@ -828,7 +1010,7 @@ int chain_va(int dtype, void *C, const void *B, long N, int num_gemm, va_list ap
         M[i] = va_arg(ap, long);
         K[i] = va_arg(ap, long);
     }
-    return host_chain(dtype, C, B, N, num_gemm, A.data(), M.data(), K.data());
+    return host_chain(dtype, C, B, N, num_gemm, A.data(), M.data(), K.data(), N, N);
 }
 
 // ---------------------------------------------------------------- SGEMM
@@ -1232,6 +1414,67 @@ FG_EXPORT int fg_sync(void)
     if (code)
         return fail(FG_ERR_TIMEOUT, "fg_chain_bf16_noalloc: a kernel's pipeline wait ran out "
                                     "(code 0x%x)", code);
+    return ok();
+}
+
+// Columns [c0, c1) of N that part `index` of `parts` owns when one chain is
+// split: whole 32-column panels (the reference's between-stage permutation
+// never crosses one), as even as the panel count allows, the first parts one
+// panel larger.
+FG_EXPORT int fg_split_columns(long N, int parts, int index, long *c0, long *c1)
+{
+    if (N < 0 || parts < 1 || index < 0 || index >= parts || !c0 || !c1)
+        return fail(FG_ERR_INVALID, "bad split arguments");
+    const long panels = (N + 31) / 32;
+    const long per = panels / parts, extra = panels % parts;
+    const long p0 = index * per + std::min<long>(index, extra);
+    const long p1 = p0 + per + (index < extra ? 1 : 0);
+    *c0 = std::min(p0 * 32, N);
+    *c1 = std::min(p1 * 32, N);
+    return ok();
+}
+
+FG_EXPORT int fg_chain_multi_device(int dtype, void *C, const void *B, long N, int num_gemm,
+                                    const void *const *A, const long *M, const long *K, int ndev,
+                                    const int *devices)
+{
+    if (dtype != FG_DT_F32 && dtype != FG_DT_BF16 && dtype != FG_DT_INT8)
+        return fail(FG_ERR_INVALID, "unknown dtype %d", dtype);
+    if (!C || !B || !A || !M || !K || !devices || ndev < 1 || ndev > 64)
+        return fail(FG_ERR_INVALID, "null pointer or bad device count");
+    int st = check_shapes(dtype, N, num_gemm, M, K);
+    if (st) return st;
+    for (int i = 0; i < num_gemm; ++i)
+        if (K[i] % 2 != 0) return fail(FG_ERR_INVALID, "gemm %d: K must be a multiple of 2", i + 1);
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(FG_ERR_NO_DEVICE, "no CUDA device");
+    }
+    for (int d = 0; d < ndev; ++d)
+        if (devices[d] < 0 || devices[d] >= count)
+            return fail(FG_ERR_INVALID, "device %d out of range (%d devices)", devices[d], count);
+    const int elt = elt_of(dtype);
+    // every part on its own host thread, its device current there; C's slices
+    // are disjoint, so the parts share nothing but the caller's read-only inputs
+    std::vector<int> status(ndev, FG_OK);
+    std::vector<std::string> msg(ndev);
+    std::vector<std::thread> th;
+    for (int d = 0; d < ndev; ++d) {
+        long c0 = 0, c1 = 0;
+        fg_split_columns(N, ndev, d, &c0, &c1);
+        if (c1 <= c0) continue;
+        th.emplace_back([&, d, c0, c1] {
+            cudaSetDevice(devices[d]);
+            status[d] = host_chain(dtype, static_cast<char *>(C) + c0 * 4,
+                                   static_cast<const char *>(B) + c0 * elt, c1 - c0, num_gemm, A, M,
+                                   K, N, N);
+            if (status[d]) msg[d] = t_msg;
+        });
+    }
+    for (auto &t : th) t.join();
+    for (int d = 0; d < ndev; ++d)
+        if (status[d]) return fail(status[d], "device %d: %s", devices[d], msg[d].c_str());
     return ok();
 }
 

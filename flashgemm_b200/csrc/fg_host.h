@@ -6,9 +6,12 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <condition_variable>
 #include <cstdint>
 #include <cstdio>
+#include <memory>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "../../include/flashgemm.h"
@@ -60,6 +63,32 @@ int tf32_chunk_blocks(long K);
 inline long round_up(long x, long a) { return (x + a - 1) / a * a; }
 inline bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
 
+// ---------------------------------------------------------------- host copies
+
+// Pitched host-to-host copies split by rows over a few threads (the caller's
+// among them): how pageable operands move to and from pinned staging memory
+// fast enough to keep the copy engines and the GPU busy.
+class RowCopier {
+public:
+    explicit RowCopier(int threads);
+    ~RowCopier();
+    void copy(void *dst, size_t dpitch, const void *src, size_t spitch, size_t width,
+              size_t height);
+
+private:
+    void run(int part);
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_go_, cv_done_;
+    unsigned long long gen_ = 0;
+    int pending_ = 0;
+    bool stop_ = false;
+    char *dst_ = nullptr;
+    const char *src_ = nullptr;
+    size_t dpitch_ = 0, spitch_ = 0, width_ = 0, height_ = 0;
+    int parts_ = 1;
+};
+
 // ---------------------------------------------------------------- per-device context
 
 struct DevCtx {
@@ -77,6 +106,12 @@ struct DevCtx {
     static constexpr int kCopyChunks = 4;
     cudaStream_t stream_h2d = nullptr, stream_d2h = nullptr;
     cudaEvent_t ev_up[kCopyChunks] = {}, ev_done[kCopyChunks] = {};
+    cudaEvent_t ev_down[kCopyChunks] = {};  // a chunk of C reached pinned staging
+    // pageable host operands: staged through this pinned buffer (grow-only) by
+    // the copier's threads
+    char *pin = nullptr;
+    size_t pin_cap = 0;
+    std::unique_ptr<RowCopier> copier;
     std::mutex mu;
     char *arena = nullptr;
     size_t arena_cap = 0;

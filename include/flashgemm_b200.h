@@ -263,6 +263,25 @@ int fg_server_destroy(fg_server s);
  * caller's stream has finished that call. */
 int fg_sync(void);
 
+/* One chain split across GPUs, no collective. No counterpart in the reference,
+ * which splits N across the OpenMP threads of one call (flashgemm.c:40-52,
+ * :109-123); here the parts are devices. The arguments are those of the
+ * reference entry points (host pointers; A, M, K as arrays of num_gemm) plus
+ * the devices to use. Columns are cut on 32-column panel boundaries
+ * (fg_split_columns), so every part runs the unchanged chain on its slice of B
+ * and writes its slice of C, and the result is bit for bit the single-device
+ * one. Blocking; one host thread per part. A device listed twice runs its
+ * parts one after the other. */
+int fg_chain_multi_device(int dtype, void *C, const void *B, long N, int num_gemm,
+                          const void *const *A, const long *M, const long *K, int ndev,
+                          const int *devices);
+
+/* Columns [*c0, *c1) of N that part `index` of `parts` owns in
+ * fg_chain_multi_device (and a rank of `parts` ranks in a column-partitioned
+ * run): whole 32-column panels, as even as the panel count allows. Host
+ * arithmetic only; needs no device. */
+int fg_split_columns(long N, int parts, int index, long *c0, long *c1);
+
 /* Self-test of failure detection; no counterpart in the reference (whose
  * only error path is print-and-return). Runs a small fused BF16 chain in which
  * the second stage waits on a dependency that nothing releases, with every

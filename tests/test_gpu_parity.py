@@ -409,3 +409,45 @@ def test_grouped_launch_matches_chains_run_alone(fg, dt):
         np.testing.assert_array_equal(c2.cpu().numpy(), c1.cpu().numpy())
         for w in W:
             w.release()
+
+
+# ---------------------------------------------------------------- one chain split across devices
+
+@pytest.mark.parametrize("dt", ["int8", "bf16", "f32"])
+@pytest.mark.parametrize("parts", [1, 3])
+def test_chain_split_across_devices_equals_one_device(fg, dt, parts):
+    """fg_chain_multi_device cuts the columns on 32-column panel boundaries and
+    runs the unchanged chain on every slice; listing device 0 several times
+    runs the parts one after another on this GPU. The result equals the
+    single-call result bit for bit."""
+    N, K1, Ms = 1312, 256, [384, 136, 100]
+    B, As, Ks = oracle.chain_inputs(dt, N, K1, Ms, seed=55)
+    one = run_chain(fg, dt, B, As, N, Ms, Ks)
+    C = np.zeros_like(one)
+    fg.chain_multi_device(dt, C, B, N, As, Ms, Ks, devices=[0] * parts)
+    rows = (Ms[-1] // 4) * 4 if dt == "int8" else Ms[-1]
+    np.testing.assert_array_equal(C[:rows], one[:rows])
+    if dt != "f32":
+        assert_parity(dt, C, oracle.chain(dt, B, As, N, Ms, Ks, mode=oracle.REF, threads=1), rows)
+
+
+@pytest.mark.parametrize("dt", ["int8", "bf16"])
+def test_pinned_and_pageable_host_buffers_give_the_same_result(fg, dt):
+    """Host operands in page-locked memory are copied directly; ordinary
+    (pageable) ones pass through the library's pinned staging, chunk by chunk.
+    Both, and a mix of the two, give the same result."""
+    import torch
+    N, K1, Ms = 2080, 256, [512, 136, 100]   # chunked (N >= 1024), last chunk narrower
+    B, As, Ks = oracle.chain_inputs(dt, N, K1, Ms, seed=66)
+    pageable = run_chain(fg, dt, B, As, N, Ms, Ks)
+    def pin(a):
+        a = np.ascontiguousarray(a)
+        v = a.view(np.int16) if a.dtype == np.uint16 else a
+        return torch.from_numpy(v).pin_memory().numpy().view(a.dtype)
+    odt = np.int32 if dt == "int8" else np.float32
+    for pb, pa, pc in [(True, True, True), (True, False, False), (False, True, True)]:
+        Bx = pin(B) if pb else B
+        Ax = [pin(a) for a in As] if pa else As
+        Cx = pin(np.zeros((Ms[-1], N), odt)) if pc else np.zeros((Ms[-1], N), odt)
+        got = run_chain(fg, dt, Bx, Ax, N, Ms, Ks, C=Cx)
+        np.testing.assert_array_equal(got, pageable)

@@ -1,8 +1,10 @@
 """The N > 1 path on CPU: two gloo ranks split one chain by activation
-columns (flashgemm_b200.shard_columns), each computes its slice with the
-reference semantics, and the gathered slices equal the unsplit chain bit for
-bit. This is the partitioning the GPU ranks use: no data-path collective, the
-all_gather here only assembles the answer for the check."""
+columns with the library's own partition (fg_split_columns, through
+flashgemm_b200.shard_columns; host arithmetic that needs no GPU, the same one
+fg_chain_multi_device and the column-partitioned bench ranks use), each
+computes its slice with the reference semantics, and the gathered slices equal
+the unsplit chain bit for bit. No data-path collective: the all_gather here
+only assembles the answer for the check."""
 import os
 import socket
 
