@@ -365,7 +365,7 @@ def group_host_inputs(specs, indices, seed):
     return out
 
 
-def run_groups(args, world, rank, local_rank, g=None):
+def run_groups(args, world, rank, local_rank, ctx=None):
     """Grouped FP32 chains. g: the shared GPU context (None: the reference arm).
     Returns the line (a dict) on rank 0 of our arm, else None."""
     seed = 4321
@@ -397,7 +397,7 @@ def run_groups(args, world, rank, local_rank, g=None):
                 "e2e": {"value": tf, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
 
-    torch, fg, dist, dev = g.torch, g.fg, g.dist, g.dev
+    torch, fg, dist, dev = ctx.torch, ctx.fg, ctx.dist, ctx.dev
     # operands: weights registered once (resident), activations and outputs in HBM;
     # chain j draws from seed + j (+ rank offset), on the device
     chains = []
@@ -420,7 +420,7 @@ def run_groups(args, world, rank, local_rank, g=None):
         chains.append((C, B, N, W))
     t_gen = time.perf_counter() - t_gen
     weight_bytes = sum(w.nbytes for c in chains for w in c[3])
-    flush = g.flush
+    flush = ctx.flush
 
     def timed(plan, sampler=None):
         for _ in range(max(args.warmup, 3)):
@@ -699,7 +699,7 @@ def serve_cpu_inputs(sets, reqs, seed):
     return host
 
 
-def run_serve(args, world, rank, local_rank, g=None):
+def run_serve(args, world, rank, local_rank, ctx=None):
     """Serving loop at fractions of its measured capacity. g: the shared GPU
     context (None: the reference arm). Returns the line on rank 0, else None."""
     seed = 777
@@ -730,7 +730,7 @@ def run_serve(args, world, rank, local_rank, g=None):
                 "e2e": {"value": tf, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
 
-    torch, fg, dist, dev = g.torch, g.fg, g.dist, g.dev
+    torch, fg, dist, dev = ctx.torch, ctx.fg, ctx.dist, ctx.dev
     fg.set_semantics("ref")
     fg.set_f32_algo("3xtf32")
     tdt = {"bf16": torch.bfloat16, "int8": torch.int8, "f32": torch.float32}
@@ -1045,14 +1045,27 @@ def run_chain_bench(args, g, workload, peaks_run=None):
                      device=dev)
     flush = g.flush
 
+    registered = None
     if dt == "f32":
         def step():
             fg.sgemm_dev(tC, tA[0], tB, Ms[0], N, K1, "ffma")
         kind = fg.FG_PK_FFMA
+    elif dt == "int8":
+        # weights resident as a server holds them: registered once (the reference's
+        # INT8 tail rows prepared at registration); fg_chain_dev on unregistered
+        # weights, which prepares them on every call, is timed beside it
+        registered = [fg.Weights(dt, a) for a in tA]
+
+        def step():
+            fg.chain_registered(dt, tC, tB, N, registered)
+        kind = fg.FG_PK_TC_I8
+        config["weights"] = ("registered once (fg_weights_register: resident in HBM, INT8 tail "
+                             "rows prepared at registration); value_unregistered: fg_chain_dev "
+                             "preparing them on every call")
     else:
         def step():
             fg.chain_dev(dt, tC, tB, N, tA, Ms, Ks)
-        kind = fg.FG_PK_TC_BF16 if dt == "bf16" else fg.FG_PK_TC_I8
+        kind = fg.FG_PK_TC_BF16
 
     for _ in range(max(args.warmup, 3)):
         step()
@@ -1094,6 +1107,14 @@ def run_chain_bench(args, g, workload, peaks_run=None):
 
     sampler = ClockSampler(torch.cuda.current_device())
     total_ms, t_wall, launches, (k_ms, k_n, k_fl) = timed(step, sampler, prof=True)
+
+    unreg = None
+    if registered is not None:
+        def step_unreg():
+            fg.chain_dev(dt, tC, tB, N, tA, Ms, Ks)
+        for _ in range(max(args.warmup, 3)):
+            step_unreg()
+        unreg, _, _, _ = timed(step_unreg)
 
     # the same steps through the plain per-GEMM path (one launch per GEMM)
     per_gemm = None
@@ -1141,6 +1162,8 @@ def run_chain_bench(args, g, workload, peaks_run=None):
     if per_gemm:
         per_gemm = (g.max_over_ranks(per_gemm[0])[0], per_gemm[1])
     cublas, = g.max_over_ranks(cublas)
+    if unreg is not None:
+        unreg, = g.max_over_ranks(unreg)
     step_flops = flops_of(N, K1, Ms)
     # whole-job work per step: every rank's columns (weak: N each; strong: one chain)
     job_flops = flops_of(N_all, K1, Ms) if strong else world * step_flops
@@ -1182,6 +1205,9 @@ def run_chain_bench(args, g, workload, peaks_run=None):
     d2h = hC.nbytes
     del hB, hA, hC, pB, pA, pC
 
+    if registered is not None:
+        for w in registered:
+            w.release()
     if rank != 0:
         return None
     peaks, peak_src = load_peaks()
@@ -1235,7 +1261,9 @@ def run_chain_bench(args, g, workload, peaks_run=None):
                     "pageable_value": e2e_pageable,
                     "pageable_api": "the same calls on ordinary (pageable) host buffers"},
             "roofline": roofline, "wall_s_timed_region": t_wall}
-    if per_gemm:
+    if unreg is not None:
+        line["value_unregistered"] = job_flops * args.steps / (unreg / 1e3) / 1e12
+        line["ms_per_step_unregistered"] = unreg / args.steps
         pg_value = job_flops * args.steps / (per_gemm[0] / 1e3) / 1e12
         line["per_gemm"] = {"value": pg_value, "unit": "TFLOP/s",
                             "ms_per_step": per_gemm[0] / args.steps,

@@ -811,8 +811,11 @@ int pin_reserve(DevCtx *c, size_t bytes)
     }
     c->pin_cap = cap;
     if (!c->copier) {
+        // FG_COPY_THREADS overrides the count (default: half the host's threads, at most 8)
+        const char *v = getenv("FG_COPY_THREADS");
         const unsigned hw = std::thread::hardware_concurrency();
-        c->copier.reset(new RowCopier((int)std::max(1u, std::min(8u, hw / 2))));
+        const int n = v ? atoi(v) : (int)std::max(1u, std::min(8u, hw / 2));
+        c->copier.reset(new RowCopier(std::max(1, std::min(64, n))));
     }
     return FG_OK;
 }

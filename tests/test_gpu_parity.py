@@ -8,9 +8,10 @@ an FP64 evaluation for accuracy statements.
 
 Tolerances (stated per dtype, as in the contract for this path):
   INT8  bit-exact against the reference semantics;
-  BF16  relative Frobenius error <= 1e-2 against the reference semantics
-        (observed ~1e-3: FP32 accumulation order differs from vdpbf16ps, which
-        flips a few BF16 roundings between stages);
+  BF16  relative Frobenius error <= 2e-3 against the reference semantics
+        (at most 6.3e-4 measured over every chain and reference shape of these
+        tests: FP32 accumulation order differs from vdpbf16ps, which flips a
+        few BF16 roundings between stages);
   FP32  plain-FMA kernel bit-exact; 3xTF32 within 2x the plain kernel's own
         error against FP64.
 """
@@ -21,7 +22,7 @@ import oracle
 
 pytestmark = pytest.mark.gpu
 
-BF16_TOL = 1e-2
+BF16_TOL = 2e-3
 
 
 @pytest.fixture(scope="module", autouse=True)
