@@ -721,7 +721,7 @@ RowCopier::~RowCopier()
 {
     {
         std::lock_guard<std::mutex> lk(mu_);
-        stop_ = true;
+        stop_.store(true);
     }
     cv_go_.notify_all();
     for (auto &t : th_) t.join();
@@ -738,22 +738,33 @@ void copy_part(char *dst, size_t dpitch, const char *src, size_t spitch, size_t 
     }
     for (size_t r = r0; r < r1; ++r) memcpy(dst + r * dpitch, src + r * spitch, width);
 }
+
+// Spin this long for the next piece before sleeping: the pieces of one call
+// follow each other within microseconds, and a sleeping worker's wake-up costs
+// tens of microseconds.
+constexpr int kSpinUs = 200;
 }  // namespace
 
 void RowCopier::run(int part)
 {
     unsigned long long seen = 0;
     while (true) {
-        {
-            std::unique_lock<std::mutex> lk(mu_);
-            cv_go_.wait(lk, [&] { return stop_ || gen_ != seen; });
-            if (stop_) return;
-            seen = gen_;
+        const auto t0 = std::chrono::steady_clock::now();
+        while (gen_.load(std::memory_order_acquire) == seen && !stop_.load()) {
+            if (std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(kSpinUs)) {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_go_.wait(lk, [&] { return stop_.load() || gen_.load() != seen; });
+                break;
+            }
         }
+        if (stop_.load()) return;
+        seen = gen_.load(std::memory_order_acquire);
         copy_part(dst_, dpitch_, src_, spitch_, width_, height_ * part / parts_,
                   height_ * (part + 1) / parts_);
-        std::lock_guard<std::mutex> lk(mu_);
-        if (--pending_ == 0) cv_done_.notify_one();
+        if (pending_.fetch_sub(1, std::memory_order_acq_rel) == 1) {
+            std::lock_guard<std::mutex> lk(mu_);
+            cv_done_.notify_one();
+        }
     }
 }
 
@@ -766,21 +777,28 @@ void RowCopier::copy(void *dst, size_t dpitch, const void *src, size_t spitch, s
         copy_part(d, dpitch, sp, spitch, width, 0, height);
         return;
     }
+    // the job's fields are published by the release increment of gen_
+    dst_ = d;
+    src_ = sp;
+    dpitch_ = dpitch;
+    spitch_ = spitch;
+    width_ = width;
+    height_ = height;
+    pending_.store(parts_ - 1, std::memory_order_relaxed);
     {
-        std::lock_guard<std::mutex> lk(mu_);
-        dst_ = d;
-        src_ = sp;
-        dpitch_ = dpitch;
-        spitch_ = spitch;
-        width_ = width;
-        height_ = height;
-        pending_ = parts_ - 1;
-        ++gen_;
+        std::lock_guard<std::mutex> lk(mu_);  // a worker about to sleep sees the new generation
+        gen_.fetch_add(1, std::memory_order_release);
     }
     cv_go_.notify_all();
     copy_part(d, dpitch, sp, spitch, width, 0, height / parts_);
-    std::unique_lock<std::mutex> lk(mu_);
-    cv_done_.wait(lk, [&] { return pending_ == 0; });
+    const auto t0 = std::chrono::steady_clock::now();
+    while (pending_.load(std::memory_order_acquire) != 0) {
+        if (std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(kSpinUs)) {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_done_.wait(lk, [&] { return pending_.load() == 0; });
+            break;
+        }
+    }
 }
 
 // How a host operand reaches the device: page-locked memory (or managed) is

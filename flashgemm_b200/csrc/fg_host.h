@@ -80,9 +80,9 @@ private:
     std::vector<std::thread> th_;
     std::mutex mu_;
     std::condition_variable cv_go_, cv_done_;
-    unsigned long long gen_ = 0;
-    int pending_ = 0;
-    bool stop_ = false;
+    std::atomic<unsigned long long> gen_{0};  // one per posted copy
+    std::atomic<int> pending_{0};             // workers still copying the current one
+    std::atomic<bool> stop_{false};
     char *dst_ = nullptr;
     const char *src_ = nullptr;
     size_t dpitch_ = 0, spitch_ = 0, width_ = 0, height_ = 0;

@@ -23,6 +23,9 @@ import oracle
 pytestmark = pytest.mark.gpu
 
 BF16_TOL = 2e-3
+# BF16 chain against the exact (FP64, unrounded) chain: an accuracy statement, not
+# parity; each between-stage narrowing to BF16 contributes up to 2^-9 relative
+BF16_VS_FP64 = 1e-2
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -169,7 +172,7 @@ def test_chain_math_semantics(fg, dt, shape):
     if dt == "bf16":
         Bf = oracle.bf16_to_f32(B)
         Af = [oracle.bf16_to_f32(a) for a in As]
-        assert oracle.rel_frob(got, oracle.chain_f64(Bf, Af, N, Ms, Ks)) < BF16_TOL
+        assert oracle.rel_frob(got, oracle.chain_f64(Bf, Af, N, Ms, Ks)) < BF16_VS_FP64
 
 
 @pytest.mark.parametrize("shape", [(256, 64, [48, 96, 24]), (520, 100, [130, 66]),
