@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libflashgemm_b200.so")
 SOURCES = ["fg_api.cu", "fg_gemm_tc.cu", "fg_chain_fused.cu", "fg_gemm_ffma.cu", "fg_aux.cu",
            "fg_noalloc.cu", "fg_group.cu", "fg_group_api.cu",
-           "fg_serve.cu", "fg_panel.cu"]
+           "fg_serve.cu", "fg_panel.cu", "fg_narrow.cu"]
 HEADERS = ["fg_kernels.h", "fg_ptx.cuh", "fg_tc_common.cuh", "fg_host.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

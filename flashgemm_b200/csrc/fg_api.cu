@@ -326,9 +326,32 @@ bool fused_enabled()
 }
 bool g_fused_unsupported[64];
 
+// Chains whose intermediates fit on chip (FG_NARROW=0: never).
+bool narrow_enabled()
+{
+    static const bool on = [] {
+        const char *v = getenv("FG_NARROW");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
 int launch_stages(DevCtx *c, int kind, std::vector<StageArgs> &stages, long N)
 {
     const int n = (int)stages.size();
+    if (fused_enabled() && narrow_enabled() && narrow_eligible(stages.data(), n)) {
+        // intermediates on chip; a chain whose operands the tensor maps cannot
+        // describe (unaligned rows) falls through to the fused chain
+        static thread_local NarrowArgs P;
+        int grid = 0;
+        if (plan_narrow(stages.data(), n, c->sms, P, grid) == cudaSuccess) {
+            double fl = 0.0;
+            for (auto &st : stages) fl += gemm_flops(st.M, st.N, st.K);
+            return run_kernel(c, kind, fl, "narrow chain",
+                              [&] { return launch_narrow(P, grid, c->status, c->work); });
+        }
+        cudaGetLastError();
+    }
     if (fused_enabled() && n <= chain_max_stages() && !g_fused_unsupported[c->dev & 63]) {
         const long tiles_n = (N + 255) / 256;
         std::vector<long> rows(n);

@@ -164,6 +164,45 @@ cudaError_t plan_single_group(const StageArgs *stages, const int *prev, int n, i
 cudaError_t launch_single_group(const GroupLaunch &g, const void *tables_dev, int *done,
                                 int *status, cudaStream_t s);
 
+// ------------------------------------------------------------------ narrow chains
+//
+// BF16 / INT8 chains whose intermediates have at most kNarrowRows rows keep
+// them on chip (fg_narrow.cu): one CTA per 128-column block, the first stage's
+// operands streamed through a TMA ring, each intermediate converted as the
+// reference does and written K-major into shared memory, only the last
+// stage's result stored. Any K_1, any last width.
+
+constexpr int kNarrowRows = 256;
+constexpr int kNarrowMaxStages = 8;
+
+struct alignas(64) NarrowStage {
+    CUtensorMap tm_w;    // weights, K-major boxes of 128 rows x 128 bytes
+    CUtensorMap tm_wt;   // INT8 reference tail block (else = tm_w)
+    CUtensorMap tm_out;  // last stage: the result (staged TMA stores)
+    int M, K;
+    int permute;         // the reference's panel permutation between stages
+    int tail_lo, tail_hi, tail_row0;
+    const uint8_t *w_tail;
+    long ld_w_tail;
+    int out_rows;        // last stage: rows stored (INT8 reference: 4 * floor(M / 4))
+};
+
+struct alignas(64) NarrowArgs {
+    NarrowStage st[kNarrowMaxStages];
+    CUtensorMap tm_b;    // first stage's activations (K_1 x N), MN-major boxes
+    const void *b;       // the same, for the INT8 tail correction
+    long ldb;
+    int n, N, nblocks;
+    int op;              // OperandKind
+    int *status;
+};
+
+bool narrow_eligible(const StageArgs *st, int n);
+// The launch parameters and grid of a chain's narrow launch (tensor maps kept
+// for the last few operand sets); cudaErrorNotSupported when it does not qualify.
+cudaError_t plan_narrow(const StageArgs *st, int n, int num_sms, NarrowArgs &out, int &grid);
+cudaError_t launch_narrow(NarrowArgs &P, int grid, int *status, cudaStream_t s);
+
 // ------------------------------------------------------------------ panel-resident chains
 //
 // FP32 (3xTF32) chains whose every dimension (K_1 and every M_i) is at most

@@ -1,0 +1,605 @@
+// BF16 / INT8 chains with narrow intermediates, kept on chip: the narrow chain.
+//
+// The reference runs all stages of a 32-column panel back to back on one core
+// and narrows each stage's result straight into the next stage's packed
+// operand (multigemm/src/flashgemm.c:123-148; kernel_bf16.h:356-391 rounds to
+// BF16 into the next Bc, kernel_int8.h:329-385 saturates to int8), so its
+// intermediates never leave the core. Its own test chains are of that shape:
+// wide activations (N up to 65536), deep first stages (K1 up to 8400) and
+// narrow intermediates (M_1, M_2 of 16 to 336; multigemm/test/test_bf16_3.c:14-48).
+// This kernel does the same on a B200 SM for chains whose intermediates have at
+// most kNarrowRows rows: a CTA owns a 128-column block, streams the first
+// stage's weights and activations through a TMA ring, and converts every
+// intermediate exactly as the reference does (BF16 round-to-nearest-even or
+// int8 saturation, the 2 x 32 / 4 x 32 panel permutation, the INT8 tail rows)
+// straight into shared memory, K-major, where the next stage's MMAs read it as
+// their B operand. Only the last stage's result is stored.
+//
+// Tiles are 128 weight rows x 128 columns (cta_group::1); a stage with more
+// rows runs several row tiles over the same operand. Two column blocks are in
+// flight per CTA (two operand buffers), their stages interleaved so that one
+// block's MMAs run while the other's epilogue converts. Warp 0 is the TMA
+// producer, warp 1 allocates TMEM and issues MMAs, warps 2-5 run the
+// epilogues. Every wait is bounded (fg_ptx.cuh). A CTA owns its column blocks
+// entirely, so no CTA waits on another.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "fg_tc_common.cuh"
+
+namespace fg {
+
+namespace {
+
+constexpr int kNBN = 128;               // columns per block (MMA N)
+constexpr int kNKbBytes = kNBN * 128;   // one K-major k-block of an operand: 16 KB
+constexpr int kNABytes = 128 * 128;     // one weight box: 128 rows x 128 bytes
+constexpr int kNAcc = 4;                // TMEM accumulators of 128 columns
+
+template <int OP>
+struct NarrowGeo {
+    static constexpr int elt = OP == OP_BF16 ? 2 : 1;
+    static constexpr int BK = 128 / elt;                   // k per 128-byte k-block
+    static constexpr int BOX_N = 128 / elt;                // MN-major box: 128-byte rows
+    static constexpr int NBOX = kNBN / BOX_N;              // B boxes per k-block
+    static constexpr int BOX_BYTES = BOX_N * BK * elt;     // 8 KB (BF16) / 16 KB (INT8)
+    static constexpr int B_KSTEP = (32 / elt) * 128;       // B bytes per MMA k-step (MN-major)
+    static constexpr int SLOT_BYTES = kNABytes + NBOX * BOX_BYTES;  // 32 KB
+    static constexpr int RING = OP == OP_BF16 ? 2 : 4;
+    static constexpr int XKB = kNarrowRows / BK;           // k-blocks of an intermediate
+    static constexpr int X_BYTES = XKB * kNKbBytes;        // 64 KB (BF16) / 32 KB (INT8)
+    static constexpr int X_OFF = RING * SLOT_BYTES;
+    static constexpr int STG_OFF = X_OFF + 2 * X_BYTES;
+    static constexpr int QUAD_OFF = STG_OFF + kEpiStagingBytes;  // INT8 tails: input quad 0
+    static constexpr int BAR_OFF = QUAD_OFF + 4 * kNBN;
+    static constexpr int SMEM = BAR_OFF + 256 + 1024;
+    // D F32 / S32, A BF16 / U8 (K-major), B BF16 / S8: MN-major as TMA lands the
+    // first stage's activations, K-major as the epilogue writes an intermediate
+    static constexpr uint32_t idesc_mn = OP == OP_BF16 ? make_idesc(1, 1, 1, 0, 1, kBM, kNBN)
+                                                       : make_idesc(2, 0, 1, 0, 1, kBM, kNBN);
+    static constexpr uint32_t idesc_k = OP == OP_BF16 ? make_idesc(1, 1, 1, 0, 0, kBM, kNBN)
+                                                      : make_idesc(2, 0, 1, 0, 0, kBM, kNBN);
+    static_assert(SMEM <= 232448, "shared memory per CTA");
+    static_assert(kNarrowRows % BK == 0, "intermediates hold whole k-blocks");
+};
+
+struct __align__(8) NarrowBars {
+    uint64_t wfull[4], wempty[4];            // ring (weights; first-stage activations)
+    uint64_t xready[2];                      // operand buffer holds the next stage's input
+    uint64_t acc_full[kNAcc], acc_empty[kNAcc];
+    uint64_t epi_sync;                       // the 4 epilogue warps meet (INT8 tails)
+    uint64_t mma_done;
+    uint32_t tmem_base;
+    int abort;
+};
+static_assert(sizeof(NarrowBars) <= 256, "barrier block");
+
+__device__ __forceinline__ void n_set_abort(NarrowBars *b) { *reinterpret_cast<volatile int *>(&b->abort) = 1; }
+__device__ __forceinline__ bool n_aborted(NarrowBars *b) { return *reinterpret_cast<volatile int *>(&b->abort) != 0; }
+
+// The work units of one CTA in the order every role walks them. The CTA owns
+// column blocks cta, cta + grid, ...; they alternate between the two operand
+// buffers (slot = position % 2), and the units of the two slots' current
+// blocks interleave. A unit is a whole intermediate stage (all its row tiles:
+// its epilogue overwrites the operand those tiles read, so it waits for all of
+// them) or one row tile of the last stage (written to global memory).
+struct NarrowWalk {
+    const NarrowArgs *g;
+    int nblk;
+    int pos[2], stage[2], row[2];
+    int turn;
+    __device__ void init(const NarrowArgs &args)
+    {
+        g = &args;
+        nblk = (int)blockIdx.x < args.nblocks
+                   ? (args.nblocks - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x
+                   : 0;
+        pos[0] = 0;
+        pos[1] = 1;
+        stage[0] = stage[1] = row[0] = row[1] = 0;
+        turn = 0;
+    }
+    __device__ int block_of(int j) const { return (int)blockIdx.x + j * (int)gridDim.x; }
+    __device__ static int row_tiles(int M) { return (M + 127) / 128; }
+    // Next unit: slot, block position j, stage, first row tile, row tiles.
+    __device__ bool next(int &slot, int &j, int &st, int &r0, int &nt)
+    {
+        int s = turn;
+        if (pos[s] >= nblk) s ^= 1;
+        if (pos[s] >= nblk) return false;
+        slot = s;
+        j = pos[s];
+        st = stage[s];
+        r0 = row[s];
+        const int R = row_tiles(g->st[st].M);
+        bool done_stage;
+        if (st + 1 < g->n) {
+            nt = R;
+            done_stage = true;
+        } else {
+            nt = 1;
+            done_stage = ++row[s] == R;
+        }
+        if (done_stage) {
+            row[s] = 0;
+            if (++stage[s] == g->n) {
+                stage[s] = 0;
+                pos[s] += 2;
+            }
+        }
+        turn = s ^ 1;
+        return true;
+    }
+};
+
+// Byte offset of element (k, n) in a K-major operand: 128-byte rows of
+// 128 / elt k-values per column n, 16-byte chunks swizzled over 8-row atoms
+// (the layout a TMA load with 128-byte swizzle gives a K-major operand).
+template <int ELT>
+__device__ __forceinline__ uint32_t kmaj(int k, int n)
+{
+    constexpr int KPB = 128 / ELT;
+    const int byte = (k % KPB) * ELT;
+    return (uint32_t)((k / KPB) * kNKbBytes + n * 128 + ((((byte >> 4) ^ (n & 7))) << 4) + (byte & 15));
+}
+
+// The epilogue warps meet on an mbarrier (bounded wait) rather than a named
+// barrier, so that a warp leaving on an error cannot strand the others.
+__device__ __forceinline__ bool epi_meet(NarrowBars *bars, uint32_t &ph, int lane, int *status)
+{
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&bars->epi_sync);
+    const bool ok = mbar_wait(&bars->epi_sync, ph, status, KERR_WAIT_ACC_FULL);
+    ph ^= 1;
+    return ok;
+}
+
+}  // namespace
+
+template <int OP>
+__global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_constant__ NarrowArgs g)
+{
+    using G = NarrowGeo<OP>;
+    constexpr MmaKind KIND = OP == OP_BF16 ? MmaKind::F16 : MmaKind::I8;
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+    NarrowBars *bars = reinterpret_cast<NarrowBars *>(smem + G::BAR_OFF);
+    uint8_t *ring = smem;
+    uint8_t *xbuf = smem + G::X_OFF;  // slot s at s * X_BYTES
+    uint32_t *quad = reinterpret_cast<uint32_t *>(smem + G::QUAD_OFF);
+    int *status = g.status;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int r = 0; r < G::RING; ++r) {
+            mbar_init(&bars->wfull[r], 1);
+            mbar_init(&bars->wempty[r], 1);
+        }
+        for (int s = 0; s < 2; ++s) mbar_init(&bars->xready[s], 4);
+        for (int a = 0; a < kNAcc; ++a) {
+            mbar_init(&bars->acc_full[a], 1);
+            mbar_init(&bars->acc_empty[a], 4);
+        }
+        mbar_init(&bars->epi_sync, 4);
+        mbar_init(&bars->mma_done, 1);
+        bars->abort = 0;
+        fence_mbar_init();
+    }
+    if (warp == 1) tmem_alloc(&bars->tmem_base, kNAcc * kNBN);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = bars->tmem_base;
+
+    NarrowWalk walk;
+    walk.init(g);
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ TMA producer
+        if (lane == 0) {
+            int r = 0;
+            uint32_t rph = 0;
+            uint32_t pending = 0, pending_ph = 0;
+            int slot, j, st, r0, nt;
+            while (walk.next(slot, j, st, r0, nt)) {
+                const NarrowStage &cs = g.st[st];
+                const int n0 = walk.block_of(j) * kNBN;
+                const int nkb = (cs.K + G::BK - 1) / G::BK;
+                int nvb = (g.N - n0 + G::BOX_N - 1) / G::BOX_N;  // boxes that start inside N
+                nvb = nvb < G::NBOX ? nvb : G::NBOX;
+                for (int t = 0; t < nt; ++t) {
+                    const int m0 = (r0 + t) * 128;
+                    const bool tail = cs.tail_hi > cs.tail_lo && m0 < cs.tail_hi && m0 + 128 > cs.tail_lo;
+                    const CUtensorMap *tma = tail ? &cs.tm_wt : &cs.tm_w;
+                    const int a_row = tail ? m0 - cs.tail_row0 : m0;
+                    for (int kb = 0; kb < nkb; ++kb) {
+                        if (!mbar_wait(&bars->wempty[r], rph ^ 1, status, KERR_WAIT_EMPTY)) {
+                            n_set_abort(bars);
+                            goto producer_done;
+                        }
+                        uint8_t *slotp = ring + r * G::SLOT_BYTES;
+                        const uint32_t tx = kNABytes + (st == 0 ? nvb * G::BOX_BYTES : 0);
+                        mbar_arrive_expect_tx(&bars->wfull[r], tx);
+                        tma_load_2d(slotp, tma, &bars->wfull[r], kb * G::BK, a_row);
+                        if (st == 0)
+                            for (int jb = 0; jb < nvb; ++jb)
+                                tma_load_2d(slotp + kNABytes + jb * G::BOX_BYTES, &g.tm_b,
+                                            &bars->wfull[r], n0 + jb * G::BOX_N, kb * G::BK);
+                        pending |= 1u << r;
+                        pending_ph = (pending_ph & ~(1u << r)) | (rph << r);
+                        if (++r == G::RING) {
+                            r = 0;
+                            rph ^= 1;
+                        }
+                    }
+                }
+                if (n_aborted(bars)) break;
+            }
+        producer_done:
+            for (int i = 0; i < G::RING; ++i)
+                if (pending & (1u << i))
+                    mbar_wait(&bars->wfull[i], (pending_ph >> i) & 1u, status, KERR_WAIT_FULL);
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            int r = 0;
+            uint32_t rph = 0;
+            unsigned tiles = 0;      // tiles issued: accumulator tiles % kNAcc, phase (tiles / kNAcc) & 1
+            int xr[2] = {0, 0};      // stage inputs consumed per slot: the xready phase
+            int slot, j, st, r0, nt;
+            while (walk.next(slot, j, st, r0, nt)) {
+                const NarrowStage &cs = g.st[st];
+                if (st > 0 && r0 == 0) {
+                    if (!mbar_wait(&bars->xready[slot], (uint32_t)(xr[slot] & 1), status,
+                                   KERR_WAIT_FULL)) {
+                        n_set_abort(bars);
+                        goto mma_done;
+                    }
+                    ++xr[slot];
+                    tc_fence_after();
+                }
+                const int nkb = (cs.K + G::BK - 1) / G::BK;
+                const uint32_t xb = smem_u32(xbuf + slot * G::X_BYTES);
+                for (int t = 0; t < nt; ++t, ++tiles) {
+                    const int acc = (int)(tiles % kNAcc);
+                    if (!mbar_wait(&bars->acc_empty[acc], ((tiles / kNAcc) & 1u) ^ 1u, status,
+                                   KERR_WAIT_ACC_EMPTY)) {
+                        n_set_abort(bars);
+                        goto mma_done;
+                    }
+                    tc_fence_after();
+                    const uint32_t d_tmem = tmem_base + acc * kNBN;
+                    for (int kb = 0; kb < nkb; ++kb) {
+                        if (!mbar_wait(&bars->wfull[r], rph, status, KERR_WAIT_FULL)) {
+                            n_set_abort(bars);
+                            goto mma_done;
+                        }
+                        tc_fence_after();
+                        const uint32_t a_addr = smem_u32(ring + r * G::SLOT_BYTES);
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const uint64_t ad = smem_desc(a_addr + k * 32, 16, 1024, SMEM_SW128);
+                            if (st == 0) {
+                                const uint64_t bd = smem_desc(a_addr + kNABytes + k * G::B_KSTEP,
+                                                              G::BOX_BYTES, 1024, SMEM_SW128);
+                                tc_mma<KIND>(d_tmem, ad, bd, G::idesc_mn, (kb | k) != 0);
+                            } else {
+                                const uint64_t bd =
+                                    smem_desc(xb + kb * kNKbBytes + k * 32, 16, 1024, SMEM_SW128);
+                                tc_mma<KIND>(d_tmem, ad, bd, G::idesc_k, (kb | k) != 0);
+                            }
+                        }
+                        tc_commit(&bars->wempty[r]);
+                        if (++r == G::RING) {
+                            r = 0;
+                            rph ^= 1;
+                        }
+                    }
+                    tc_commit(&bars->acc_full[acc]);
+                }
+                if (n_aborted(bars)) break;
+            }
+        mma_done:
+            tc_commit(&bars->mma_done);
+            mbar_wait(&bars->mma_done, 0, status, KERR_WAIT_FULL);
+        }
+    } else {
+        // ------------------------------------------------------------ epilogues (warps 2..5)
+        const int quarter = warp & 3;
+        const int et = threadIdx.x - 64;  // 0..127: this thread's column for the tail snapshot
+        uint8_t *staging = smem + G::STG_OFF + (warp - 2) * 2 * kStageBufBytes;
+        int sbuf = 0;
+        unsigned tiles = 0;
+        uint32_t meet_ph = 0;
+        bool ok = true;
+        int slot, j, st, r0, nt;
+        while (ok && walk.next(slot, j, st, r0, nt)) {
+            const NarrowStage &cs = g.st[st];
+            const bool last = st + 1 == g.n;
+            const int n0 = walk.block_of(j) * kNBN;
+            uint8_t *xs = xbuf + slot * G::X_BYTES;
+            // every tile of the unit: an intermediate overwrites the operand they read
+            for (int t = 0; t < nt && ok; ++t) {
+                const unsigned tt = tiles + t;
+                ok = mbar_wait(&bars->acc_full[tt % kNAcc], (tt / kNAcc) & 1u, status,
+                               KERR_WAIT_ACC_FULL);
+            }
+            if (!ok) break;
+            tc_fence_after();
+            // INT8 tail rows add weight quad 0 x input quad 0; a later stage's input
+            // quad is in this slot's operand buffer, copied aside before any warp
+            // overwrites it (every warp passes the meeting points alike)
+            const bool tails = OP == OP_I8 && cs.tail_hi > cs.tail_lo;
+            if (tails && st > 0) {
+                if (!(ok = epi_meet(bars, meet_ph, lane, status))) break;
+                quad[et] = *reinterpret_cast<const uint32_t *>(xs + kmaj<1>(0, et));
+                if (!(ok = epi_meet(bars, meet_ph, lane, status))) break;
+            }
+            for (int t = 0; t < nt; ++t) {
+                const unsigned tt = tiles + t;
+                const int row = (r0 + t) * 128 + quarter * 32 + lane;  // stage output row
+                const uint32_t t_row =
+                    tmem_base + (tt % kNAcc) * kNBN + ((uint32_t)(quarter * 32) << 16);
+                const bool tail_row = tails && row >= cs.tail_lo && row < cs.tail_hi;
+                uint32_t wq = 0;
+                if (tail_row)
+                    wq = *reinterpret_cast<const uint32_t *>(
+                        cs.w_tail + (size_t)(row - cs.tail_row0) * cs.ld_w_tail + cs.K);
+                const int warp_row0 = (r0 + t) * 128 + quarter * 32;
+#pragma unroll 1
+                for (int c = 0; c < kNBN / 32; ++c) {
+                    const int lc = c * 32, nc = n0 + lc;
+                    if (nc >= g.N) break;  // warp-uniform
+                    uint32_t v[32];
+                    tmem_ld_32x32b_x32(t_row + c * 32, v);
+                    tmem_ld_wait();
+                    if (tail_row) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const int a = (int)((wq >> (8 * q)) & 0xffu);
+#pragma unroll
+                            for (int jj = 0; jj < 32; ++jj) {
+                                int x;
+                                if (st == 0)
+                                    x = nc + jj < g.N ? (int)reinterpret_cast<const int8_t *>(
+                                                            g.b)[(size_t)q * g.ldb + nc + jj]
+                                                      : 0;
+                                else
+                                    x = (int)(int8_t)((quad[lc + jj] >> (8 * q)) & 0xffu);
+                                v[jj] = (uint32_t)((int32_t)v[jj] + a * x);
+                            }
+                        }
+                    }
+                    if (last) {
+                        // the chain's result: staged TMA store of these 32 columns
+                        uint8_t *b0 = staging + sbuf * kStageBufBytes;
+                        if (lane == 0) bulk_wait_read<1>();
+                        __syncwarp();
+#pragma unroll
+                        for (int q = 0; q < 8; ++q)
+                            st_sw16(b0, lane, 16 * q,
+                                    make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]));
+                        sbuf ^= 1;
+                        fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0 && warp_row0 < cs.out_rows) {
+                            tma_store_2d(&cs.tm_out, b0, nc, warp_row0);
+                            bulk_commit();
+                        }
+                        continue;
+                    }
+                    // an intermediate: the reference's narrowing and panel permutation,
+                    // written K-major into the next stage's operand (k' = output row)
+                    const bool full = nc + 32 <= g.N;
+                    if constexpr (OP == OP_BF16) {
+                        if (cs.permute && full && row < (cs.M & ~1)) {
+                            // (2q + h, c) -> (2q + (c & 1), 16h + c / 2)  (kernel_bf16.h:6-32)
+                            const int h = row & 1, k0 = row - h;
+#pragma unroll
+                            for (int u = 0; u < 16; ++u)
+                                *reinterpret_cast<uint32_t *>(xs + kmaj<2>(k0, lc + 16 * h + u)) =
+                                    pack_bf16x2(v[2 * u], v[2 * u + 1]);
+                        } else {
+#pragma unroll
+                            for (int u = 0; u < 32; ++u)
+                                *reinterpret_cast<uint16_t *>(xs + kmaj<2>(row, lc + u)) =
+                                    (uint16_t)(pack_bf16x2(v[u], v[u]) & 0xffffu);
+                        }
+                    } else {
+                        if (cs.permute && full && row < (cs.M / 4) * 4) {
+                            // (4q + h, c) -> (4q + (c & 3), 8h + c / 4)  (kernel_int8.h:6-50)
+                            const int h = row & 3, k0 = row - h;
+#pragma unroll
+                            for (int u = 0; u < 8; ++u)
+                                *reinterpret_cast<uint32_t *>(xs + kmaj<1>(k0, lc + 8 * h + u)) =
+                                    pack_s8x4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
+                        } else {
+#pragma unroll
+                            for (int u = 0; u < 32; ++u)
+                                xs[kmaj<1>(row, lc + u)] = (uint8_t)(pack_s8x4(v[u], 0, 0, 0) & 0xffu);
+                        }
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bars->acc_empty[tt % kNAcc]);
+            }
+            tiles += nt;
+            if (!last) {
+                // the next stage's input is in place: tell the MMA warp
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bars->xready[slot]);
+            }
+            if (n_aborted(bars)) break;
+        }
+        if (!ok) n_set_abort(bars);
+    }
+
+    if (warp >= 2 && lane == 0) bulk_wait<0>();
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        __syncwarp();
+        tc_fence_after();
+        tmem_dealloc(tmem_base, kNAcc * kNBN);
+    }
+}
+
+// ------------------------------------------------------------------ host side
+
+bool narrow_eligible(const StageArgs *st, int n)
+{
+    if (n < 2 || n > kNarrowMaxStages) return false;
+    const int op = st[0].op;
+    if (op != OP_BF16 && op != OP_I8) return false;
+    const long N = st[0].N;
+    if (N < 1 || (N + kNBN - 1) / kNBN > (1l << 30)) return false;
+    for (int i = 0; i < n; ++i) {
+        if (st[i].op != op || st[i].N != N) return false;
+        if (i + 1 < n && (st[i].M > kNarrowRows || st[i].M < 1)) return false;
+    }
+    return true;
+}
+
+namespace {
+
+template <int OP>
+cudaError_t narrow_capacity(int &per_sm)
+{
+    using G = NarrowGeo<OP>;
+    static std::mutex mu;
+    static unsigned long long known = 0;
+    static int cap[64];
+    std::lock_guard<std::mutex> lk(mu);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(known & (1ull << (dev & 63)))) {
+        cudaError_t e = cudaFuncSetAttribute(tc_narrow_kernel<OP>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+        if (e != cudaSuccess) return e;
+        int n = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tc_narrow_kernel<OP>, kThreads, G::SMEM);
+        if (e != cudaSuccess || n < 1) {
+            cudaGetLastError();
+            return cudaErrorNotSupported;
+        }
+        cap[dev & 63] = n;
+        known |= 1ull << (dev & 63);
+    }
+    per_sm = cap[dev & 63];
+    return cudaSuccess;
+}
+
+template <int OP>
+cudaError_t plan_narrow_op(const StageArgs *st, int n, int num_sms, NarrowArgs &out, int &grid)
+{
+    using G = NarrowGeo<OP>;
+    const CUtensorMapDataType dt = OP == OP_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                 : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+    // parameter blocks of the last few operand sets (tensor maps encoded once)
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    struct Built {
+        std::vector<long> key;
+        NarrowArgs P;
+    };
+    static std::vector<Built *> built;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::vector<long> key = {dev, num_sms, n};
+    for (int i = 0; i < n; ++i) {
+        const StageArgs &a = st[i];
+        const long v[] = {a.M, a.N, a.K, (long)a.w, a.ld_w, (long)a.x, a.ld_x, a.epi, (long)a.out,
+                          a.ld_out, a.permute, a.m_written, a.tail_lo, a.tail_hi,
+                          (long)a.w_tail, a.ld_w_tail, a.tail_row0};
+        key.insert(key.end(), std::begin(v), std::end(v));
+    }
+    NarrowArgs *P = nullptr;
+    for (size_t i = 0; i < built.size(); ++i)
+        if (built[i]->key == key) {
+            Built *b = built[i];
+            built.erase(built.begin() + i);
+            built.push_back(b);
+            P = &b->P;
+            break;
+        }
+    if (!P) {
+        std::unique_ptr<Built> b(new Built);
+        memset(&b->P, 0, sizeof b->P);
+        NarrowArgs &A = b->P;
+        if (!make_map(&A.tm_b, dt, G::elt, st[0].x, st[0].K, st[0].N, st[0].ld_x, G::BOX_N, G::BK))
+            return cudaErrorNotSupported;
+        for (int i = 0; i < n; ++i) {
+            const StageArgs &a = st[i];
+            NarrowStage &cs = A.st[i];
+            if (!make_map(&cs.tm_w, dt, G::elt, a.w, a.M, a.K, a.ld_w, G::BK, 128))
+                return cudaErrorNotSupported;
+            cs.tm_wt = cs.tm_w;
+            if (a.tail_hi > a.tail_lo &&
+                !make_map(&cs.tm_wt, dt, G::elt, a.w_tail, a.M - a.tail_row0, a.K, a.ld_w_tail,
+                          G::BK, 128))
+                return cudaErrorNotSupported;
+            cs.M = a.M;
+            cs.K = a.K;
+            cs.permute = a.permute;
+            cs.tail_lo = a.tail_lo;
+            cs.tail_hi = a.tail_hi;
+            cs.tail_row0 = a.tail_row0;
+            cs.w_tail = static_cast<const uint8_t *>(a.w_tail);
+            cs.ld_w_tail = a.ld_w_tail;
+            cs.out_rows = a.m_written;
+            if (i + 1 == n && !make_out_map(&cs.tm_out, a)) return cudaErrorNotSupported;
+            if (i + 1 < n) cs.tm_out = cs.tm_w;
+        }
+        A.b = st[0].x;
+        A.ldb = st[0].ld_x;
+        A.op = OP;
+        A.n = n;
+        A.N = st[0].N;
+        A.nblocks = (st[0].N + kNBN - 1) / kNBN;
+        b->key.swap(key);
+        if (built.size() >= 8) {
+            delete built.front();
+            built.erase(built.begin());
+        }
+        built.push_back(b.release());
+        P = &built.back()->P;
+    }
+    int per_sm = 0;
+    cudaError_t e = narrow_capacity<OP>(per_sm);
+    if (e != cudaSuccess) return e;
+    out = *P;  // a copy: the cache may drop this entry once the lock is released
+    grid = std::min(P->nblocks, per_sm * num_sms);
+    return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t plan_narrow(const StageArgs *st, int n, int num_sms, NarrowArgs &out, int &grid)
+{
+    if (!narrow_eligible(st, n)) return cudaErrorNotSupported;
+    return st[0].op == OP_BF16 ? plan_narrow_op<OP_BF16>(st, n, num_sms, out, grid)
+                               : plan_narrow_op<OP_I8>(st, n, num_sms, out, grid);
+}
+
+cudaError_t launch_narrow(NarrowArgs &P, int grid, int *status, cudaStream_t s)
+{
+    P.status = status;
+    if (P.op == OP_BF16)
+        tc_narrow_kernel<OP_BF16><<<grid, kThreads, NarrowGeo<OP_BF16>::SMEM, s>>>(P);
+    else
+        tc_narrow_kernel<OP_I8><<<grid, kThreads, NarrowGeo<OP_I8>::SMEM, s>>>(P);
+    return cudaGetLastError();
+}
+
+}  // namespace fg
