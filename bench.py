@@ -712,7 +712,9 @@ def run_serve(args, world, rank, local_rank, ctx=None):
                           "activations and results resident in HBM",
               "requests_per_rate": nreq, "weight_sets": len(sets),
               "server": {"max_batch": 64, "slots": 2, "max_wait_us": 200,
-                         "max_queue_us": args.serve_deadline_us},
+                         "max_queue_us": f"{args.serve_deadline_us} at offered rates above "
+                                         "capacity; 0 (no shedding) at or below it and for "
+                                         "the capacity bursts"},
               "l2": "inputs of the stream far exceed L2; no flush between requests",
               "parallelism": f"dp{world} (each rank serves its own stream)"}
     metric = "served chain requests TFLOP/s (p50/p99 latency beside)"
@@ -773,7 +775,12 @@ def run_serve(args, world, rank, local_rank, ctx=None):
             out.append((dt, W[i], Bs[i][:K1 * N].view(K1, N), c[:Ms[-1] * N].view(Ms[-1], N)))
         return out
 
-    srv = fg.Server(max_batch=64, slots=2, max_wait_us=200, max_queue_us=args.serve_deadline_us)
+    # capacity and the points at or below it on a server that never sheds (a burst
+    # queues every request at once, far past any deadline); the overload points on
+    # one that sheds requests still queued args.serve_deadline_us after submit
+    plain_srv = fg.Server(max_batch=64, slots=2, max_wait_us=200)
+    shed_srv = None
+    srv = plain_srv
 
     def run_point(reqs, at_us, prof=False):
         if dist:
@@ -815,6 +822,13 @@ def run_serve(args, world, rank, local_rank, ctx=None):
     rng = np.random.default_rng(seed + 3)
     with sampler:
         for k, frac in enumerate(args.serve_rates):
+            if frac > 1.0 and args.serve_deadline_us > 0:
+                if shed_srv is None:
+                    shed_srv = fg.Server(max_batch=64, slots=2, max_wait_us=200,
+                                         max_queue_us=args.serve_deadline_us)
+                srv = shed_srv
+            else:
+                srv = plain_srv
             rate = frac * capacity
             reqs = serve_requests(seed + 10 + k, sets, nreq)
             at = np.cumsum(rng.exponential(1e6 / rate, size=nreq))
@@ -852,13 +866,16 @@ def run_serve(args, world, rank, local_rank, ctx=None):
         d2h += c.nbytes
     rate = 0.6 * capacity
     at = np.cumsum(rng.exponential(1e6 / rate, size=e2e_n))
+    srv = plain_srv
     srv.reset_stats()
     ids = srv.replay(mats, at.tolist())
     srv.drain()
     st_e2e = srv.stats()
     for rid in ids:
         srv.wait(rid, shed_ok=True)
-    srv.close()
+    plain_srv.close()
+    if shed_srv is not None:
+        shed_srv.close()
     for ws in W:
         for w in ws:
             w.release()
