@@ -280,6 +280,9 @@ size_t chain_scratch(int dtype, int algo, long N, int n, const long *M, const lo
             size_t items = 0;
             for (int i = 0; i < n; ++i) items += (size_t)((M[i] + 255) / 256) * ((N + 255) / 256);
             s += carve_size(items * 2 * 10 * 8);
+            // or of the narrow kernel: one row per (column block, unit) at most
+            s += carve_size((size_t)((N + 127) / 128) * (n - 1 + (M[n - 1] + 127) / 128) *
+                            kNarrowTraceFields * 8);
         }
     }
     if (dtype == FG_DT_INT8) {
@@ -347,8 +350,43 @@ int launch_stages(DevCtx *c, int kind, std::vector<StageArgs> &stages, long N)
         if (plan_narrow(stages.data(), n, c->sms, P, grid) == cudaSuccess) {
             double fl = 0.0;
             for (auto &st : stages) fl += gemm_flops(st.M, st.N, st.K);
-            return run_kernel(c, kind, fl, "narrow chain",
-                              [&] { return launch_narrow(P, grid, c->status, c->work); });
+            // FG_TRACE_DIR=<dir>: a per-unit timeline of every narrow launch
+            static const char *trace_dir = getenv("FG_TRACE_DIR");
+            size_t trace_words = 0;
+            P.trace = nullptr;
+            if (trace_dir) {
+                P.trace_units = narrow_units_per_cta(P, grid);
+                trace_words = (size_t)grid * P.trace_units * kNarrowTraceFields;
+                P.trace = (unsigned long long *)arena_take(c, trace_words * 8);
+                CUDA_TRY(cudaMemsetAsync(P.trace, 0, trace_words * 8, c->work));
+            }
+            const int st = run_kernel(c, kind, fl, "narrow chain",
+                                      [&] { return launch_narrow(P, grid, c->status, c->work); });
+            if (st == FG_OK && P.trace) {
+                std::vector<unsigned long long> h(trace_words);
+                CUDA_TRY(cudaMemcpyAsync(h.data(), P.trace, trace_words * 8,
+                                         cudaMemcpyDeviceToHost, c->work));
+                CUDA_TRY(cudaStreamSynchronize(c->work));
+                static int seq = 0;
+                char path[1024];
+                snprintf(path, sizeof path, "%s/narrow_trace_%d.csv", trace_dir, seq++);
+                if (FILE *f = fopen(path, "w")) {
+                    fprintf(f, "cta,unit,stage,pos,row0,tiles,sm,prod_start,prod_end,mma_wait,"
+                               "mma_start,mma_end,epi_start,epi_end\n");
+                    for (size_t r = 0; r < trace_words / kNarrowTraceFields; ++r) {
+                        const unsigned long long *v = &h[r * kNarrowTraceFields];
+                        if (!v[1]) continue;  // a unit the CTA did not have
+                        fprintf(f, "%zu,%zu,%llu,%llu,%llu,%llu,%llu", r / P.trace_units,
+                                r % P.trace_units, v[0] & 0xff, (v[0] >> 8) & 0xffff,
+                                (v[0] >> 24) & 0xff, (v[0] >> 32) & 0xff, v[0] >> 40);
+                        for (int k = 1; k < kNarrowTraceFields; ++k) fprintf(f, ",%llu", v[k]);
+                        fprintf(f, "\n");
+                    }
+                    fclose(f);
+                }
+            }
+            P.trace = nullptr;
+            return st;
         }
         cudaGetLastError();
     }

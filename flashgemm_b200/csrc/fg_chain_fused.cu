@@ -94,12 +94,6 @@ __device__ __forceinline__ void trace_put(const ChainParams &P, int t, uint32_t 
     if (P.trace) P.trace[((size_t)t * 2 + rank) * kTraceFields + f] = v;
 }
 
-__device__ __forceinline__ uint32_t smid()
-{
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
-    return r;
-}
 
 // Epilogue warps per CTA (4) x CTAs per pair (2): counter increments per tile.
 constexpr int kDoneIncrementsPerTile = 8;
@@ -213,7 +207,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
                         const uint64_t t0 = globaltimer_ns();
                         while (ld_acquire_gpu(cnt) < need) {
                             __nanosleep(64);
-                            if (globaltimer_ns() - t0 > wait_limit_ns()) {
+                            if (wait_expired(t0)) {
                                 atomicCAS(status, 0, KERR_WAIT_DEPENDENCY);
                                 set_abort(bars);
                                 goto producer_done;
@@ -259,7 +253,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_chain_kernel(const __grid_cons
                             const uint64_t t0 = globaltimer_ns();
                             while (ld_acquire_gpu(row_cnt + g) < kDoneIncrementsPerTile) {
                                 __nanosleep(32);
-                                if (globaltimer_ns() - t0 > wait_limit_ns()) {
+                                if (wait_expired(t0)) {
                                     atomicCAS(status, 0, KERR_WAIT_DEPENDENCY);
                                     set_abort(bars);
                                     goto producer_done;

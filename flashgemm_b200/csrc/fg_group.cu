@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_group_kernel(const GroupArgs g
                         const uint64_t t0 = globaltimer_ns();
                         while (ld_acquire_gpu(cnt) < need) {
                             __nanosleep(64);
-                            if (globaltimer_ns() - t0 > wait_limit_ns()) {
+                            if (wait_expired(t0)) {
                                 atomicCAS(status, 0, KERR_WAIT_DEPENDENCY);
                                 set_abort(bars);
                                 goto producer_done;

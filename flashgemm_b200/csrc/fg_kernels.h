@@ -174,6 +174,7 @@ cudaError_t launch_single_group(const GroupLaunch &g, const void *tables_dev, in
 
 constexpr int kNarrowRows = 256;
 constexpr int kNarrowMaxStages = 8;
+constexpr int kNarrowMaxRing = 4;
 
 struct alignas(64) NarrowStage {
     CUtensorMap tm_w;    // weights, K-major boxes of 128 rows x 128 bytes
@@ -194,14 +195,24 @@ struct alignas(64) NarrowArgs {
     long ldb;
     int n, N, nblocks;
     int op;              // OperandKind
+    // shared memory layout of the launch: ring slots of slot_bytes (ra weight
+    // boxes, then the first stage's activation boxes), xslots operand buffers
+    // of x_bytes (1: one column block in flight, 2: two), smem bytes in all
+    int ring, slot_bytes, ra, x_bytes, xslots, smem;
     int *status;
+    // optional (else null): kNarrowTraceFields %globaltimer stamps per (CTA, unit)
+    unsigned long long *trace;
+    int trace_units;     // units per CTA the trace holds
 };
+constexpr int kNarrowTraceFields = 8;
 
 bool narrow_eligible(const StageArgs *st, int n);
 // The launch parameters and grid of a chain's narrow launch (tensor maps kept
 // for the last few operand sets); cudaErrorNotSupported when it does not qualify.
 cudaError_t plan_narrow(const StageArgs *st, int n, int num_sms, NarrowArgs &out, int &grid);
 cudaError_t launch_narrow(NarrowArgs &P, int grid, int *status, cudaStream_t s);
+// Work units one CTA of a narrow launch walks at most (the trace's rows per CTA).
+int narrow_units_per_cta(const NarrowArgs &P, int grid);
 
 // ------------------------------------------------------------------ panel-resident chains
 //

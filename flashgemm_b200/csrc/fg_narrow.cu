@@ -49,28 +49,27 @@ struct NarrowGeo {
     static constexpr int BOX_N = 128 / elt;                // MN-major box: 128-byte rows
     static constexpr int NBOX = kNBN / BOX_N;              // B boxes per k-block
     static constexpr int BOX_BYTES = BOX_N * BK * elt;     // 8 KB (BF16) / 16 KB (INT8)
+    static constexpr int B_BYTES = NBOX * BOX_BYTES;       // 16 KB
     static constexpr int B_KSTEP = (32 / elt) * 128;       // B bytes per MMA k-step (MN-major)
-    static constexpr int SLOT_BYTES = kNABytes + NBOX * BOX_BYTES;  // 32 KB
-    static constexpr int RING = OP == OP_BF16 ? 2 : 4;
-    static constexpr int XKB = kNarrowRows / BK;           // k-blocks of an intermediate
-    static constexpr int X_BYTES = XKB * kNKbBytes;        // 64 KB (BF16) / 32 KB (INT8)
-    static constexpr int X_OFF = RING * SLOT_BYTES;
-    static constexpr int STG_OFF = X_OFF + 2 * X_BYTES;
-    static constexpr int QUAD_OFF = STG_OFF + kEpiStagingBytes;  // INT8 tails: input quad 0
-    static constexpr int BAR_OFF = QUAD_OFF + 4 * kNBN;
-    static constexpr int SMEM = BAR_OFF + 256 + 1024;
     // D F32 / S32, A BF16 / U8 (K-major), B BF16 / S8: MN-major as TMA lands the
     // first stage's activations, K-major as the epilogue writes an intermediate
     static constexpr uint32_t idesc_mn = OP == OP_BF16 ? make_idesc(1, 1, 1, 0, 1, kBM, kNBN)
                                                        : make_idesc(2, 0, 1, 0, 1, kBM, kNBN);
     static constexpr uint32_t idesc_k = OP == OP_BF16 ? make_idesc(1, 1, 1, 0, 0, kBM, kNBN)
                                                       : make_idesc(2, 0, 1, 0, 0, kBM, kNBN);
-    static_assert(SMEM <= 232448, "shared memory per CTA");
     static_assert(kNarrowRows % BK == 0, "intermediates hold whole k-blocks");
 };
 
+// Shared memory of a launch (sizes per launch, NarrowArgs): the ring of slots
+// (each the weight boxes of one unit's row tiles and, for the first stage, the
+// activation boxes they share), the operand buffers (one or two blocks in
+// flight), the output staging, the INT8 tail quad, the barriers.
+constexpr int kNQuadBytes = 4 * kNBN;
+constexpr int kNFixedBytes = kEpiStagingBytes + kNQuadBytes + 256 + 1024;
+constexpr int kNMaxSmem = 232448;
+
 struct __align__(8) NarrowBars {
-    uint64_t wfull[4], wempty[4];            // ring (weights; first-stage activations)
+    uint64_t wfull[kNarrowMaxRing], wempty[kNarrowMaxRing];  // ring
     uint64_t xready[2];                      // operand buffer holds the next stage's input
     uint64_t acc_full[kNAcc], acc_empty[kNAcc];
     uint64_t epi_sync;                       // the 4 epilogue warps meet (INT8 tails)
@@ -84,14 +83,15 @@ __device__ __forceinline__ void n_set_abort(NarrowBars *b) { *reinterpret_cast<v
 __device__ __forceinline__ bool n_aborted(NarrowBars *b) { return *reinterpret_cast<volatile int *>(&b->abort) != 0; }
 
 // The work units of one CTA in the order every role walks them. The CTA owns
-// column blocks cta, cta + grid, ...; they alternate between the two operand
-// buffers (slot = position % 2), and the units of the two slots' current
+// column blocks cta, cta + grid, ...; with two operand buffers they alternate
+// between them (slot = position % 2) and the units of the two slots' current
 // blocks interleave. A unit is a whole intermediate stage (all its row tiles:
 // its epilogue overwrites the operand those tiles read, so it waits for all of
-// them) or one row tile of the last stage (written to global memory).
+// them, and they share each k-block of their B operand) or one row tile of the
+// last stage (written to global memory).
 struct NarrowWalk {
     const NarrowArgs *g;
-    int nblk;
+    int nblk, step;
     int pos[2], stage[2], row[2];
     int turn;
     __device__ void init(const NarrowArgs &args)
@@ -100,8 +100,9 @@ struct NarrowWalk {
         nblk = (int)blockIdx.x < args.nblocks
                    ? (args.nblocks - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x
                    : 0;
+        step = args.xslots;
         pos[0] = 0;
-        pos[1] = 1;
+        pos[1] = args.xslots == 2 ? 1 : (1 << 30);
         stage[0] = stage[1] = row[0] = row[1] = 0;
         turn = 0;
     }
@@ -130,13 +131,22 @@ struct NarrowWalk {
             row[s] = 0;
             if (++stage[s] == g->n) {
                 stage[s] = 0;
-                pos[s] += 2;
+                pos[s] += step;
             }
         }
         turn = s ^ 1;
         return true;
     }
 };
+
+// Timeline of a unit (FG_TRACE_DIR): its description, then the roles' stamps.
+enum { NT_DESC, NT_PROD_START, NT_PROD_END, NT_MMA_WAIT, NT_MMA_START, NT_MMA_END, NT_EPI_START,
+       NT_EPI_END };
+__device__ __forceinline__ void ntrace(const NarrowArgs &g, int u, int f, unsigned long long v)
+{
+    if (g.trace && u < g.trace_units)
+        g.trace[((size_t)blockIdx.x * g.trace_units + u) * kNarrowTraceFields + f] = v;
+}
 
 // Byte offset of element (k, n) in a K-major operand: 128-byte rows of
 // 128 / elt k-values per column n, 16-byte chunks swizzled over 8-row atoms
@@ -170,16 +180,18 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
-    NarrowBars *bars = reinterpret_cast<NarrowBars *>(smem + G::BAR_OFF);
-    uint8_t *ring = smem;
-    uint8_t *xbuf = smem + G::X_OFF;  // slot s at s * X_BYTES
-    uint32_t *quad = reinterpret_cast<uint32_t *>(smem + G::QUAD_OFF);
+    uint8_t *ring = smem;                                   // slot r at r * slot_bytes
+    uint8_t *xbuf = ring + g.ring * g.slot_bytes;           // operand s at s * x_bytes
+    uint8_t *stg0 = xbuf + g.xslots * g.x_bytes;
+    uint32_t *quad = reinterpret_cast<uint32_t *>(stg0 + kEpiStagingBytes);
+    NarrowBars *bars = reinterpret_cast<NarrowBars *>(stg0 + kEpiStagingBytes + kNQuadBytes);
     int *status = g.status;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
+    const int RING = g.ring;
 
     if (threadIdx.x == 0) {
-        for (int r = 0; r < G::RING; ++r) {
+        for (int r = 0; r < RING; ++r) {
             mbar_init(&bars->wfull[r], 1);
             mbar_init(&bars->wempty[r], 1);
         }
@@ -209,42 +221,51 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
             uint32_t rph = 0;
             uint32_t pending = 0, pending_ph = 0;
             int slot, j, st, r0, nt;
-            while (walk.next(slot, j, st, r0, nt)) {
+            for (int u = 0; walk.next(slot, j, st, r0, nt); ++u) {
                 const NarrowStage &cs = g.st[st];
                 const int n0 = walk.block_of(j) * kNBN;
                 const int nkb = (cs.K + G::BK - 1) / G::BK;
+                if (g.trace) {
+                    ntrace(g, u, NT_DESC,
+                           (unsigned long long)st | (unsigned long long)j << 8 |
+                               (unsigned long long)r0 << 24 | (unsigned long long)nt << 32 |
+                               (unsigned long long)smid() << 40);
+                    ntrace(g, u, NT_PROD_START, globaltimer_ns());
+                }
                 int nvb = (g.N - n0 + G::BOX_N - 1) / G::BOX_N;  // boxes that start inside N
                 nvb = nvb < G::NBOX ? nvb : G::NBOX;
-                for (int t = 0; t < nt; ++t) {
-                    const int m0 = (r0 + t) * 128;
-                    const bool tail = cs.tail_hi > cs.tail_lo && m0 < cs.tail_hi && m0 + 128 > cs.tail_lo;
-                    const CUtensorMap *tma = tail ? &cs.tm_wt : &cs.tm_w;
-                    const int a_row = tail ? m0 - cs.tail_row0 : m0;
-                    for (int kb = 0; kb < nkb; ++kb) {
-                        if (!mbar_wait(&bars->wempty[r], rph ^ 1, status, KERR_WAIT_EMPTY)) {
-                            n_set_abort(bars);
-                            goto producer_done;
-                        }
-                        uint8_t *slotp = ring + r * G::SLOT_BYTES;
-                        const uint32_t tx = kNABytes + (st == 0 ? nvb * G::BOX_BYTES : 0);
-                        mbar_arrive_expect_tx(&bars->wfull[r], tx);
-                        tma_load_2d(slotp, tma, &bars->wfull[r], kb * G::BK, a_row);
-                        if (st == 0)
-                            for (int jb = 0; jb < nvb; ++jb)
-                                tma_load_2d(slotp + kNABytes + jb * G::BOX_BYTES, &g.tm_b,
-                                            &bars->wfull[r], n0 + jb * G::BOX_N, kb * G::BK);
-                        pending |= 1u << r;
-                        pending_ph = (pending_ph & ~(1u << r)) | (rph << r);
-                        if (++r == G::RING) {
-                            r = 0;
-                            rph ^= 1;
-                        }
+                for (int kb = 0; kb < nkb; ++kb) {
+                    if (!mbar_wait(&bars->wempty[r], rph ^ 1, status, KERR_WAIT_EMPTY)) {
+                        n_set_abort(bars);
+                        goto producer_done;
+                    }
+                    uint8_t *slotp = ring + r * g.slot_bytes;
+                    const uint32_t tx = nt * kNABytes + (st == 0 ? nvb * G::BOX_BYTES : 0);
+                    mbar_arrive_expect_tx(&bars->wfull[r], tx);
+                    for (int t = 0; t < nt; ++t) {
+                        // the unit's row tile t: weight rows m0 .. m0 + 127
+                        const int m0 = (r0 + t) * 128;
+                        const bool tail =
+                            cs.tail_hi > cs.tail_lo && m0 < cs.tail_hi && m0 + 128 > cs.tail_lo;
+                        tma_load_2d(slotp + t * kNABytes, tail ? &cs.tm_wt : &cs.tm_w,
+                                    &bars->wfull[r], kb * G::BK, tail ? m0 - cs.tail_row0 : m0);
+                    }
+                    if (st == 0)  // the first stage's activations, shared by the row tiles
+                        for (int jb = 0; jb < nvb; ++jb)
+                            tma_load_2d(slotp + g.ra * kNABytes + jb * G::BOX_BYTES, &g.tm_b,
+                                        &bars->wfull[r], n0 + jb * G::BOX_N, kb * G::BK);
+                    pending |= 1u << r;
+                    pending_ph = (pending_ph & ~(1u << r)) | (rph << r);
+                    if (++r == RING) {
+                        r = 0;
+                        rph ^= 1;
                     }
                 }
+                if (g.trace) ntrace(g, u, NT_PROD_END, globaltimer_ns());
                 if (n_aborted(bars)) break;
             }
         producer_done:
-            for (int i = 0; i < G::RING; ++i)
+            for (int i = 0; i < RING; ++i)
                 if (pending & (1u << i))
                     mbar_wait(&bars->wfull[i], (pending_ph >> i) & 1u, status, KERR_WAIT_FULL);
         }
@@ -256,8 +277,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
             unsigned tiles = 0;      // tiles issued: accumulator tiles % kNAcc, phase (tiles / kNAcc) & 1
             int xr[2] = {0, 0};      // stage inputs consumed per slot: the xready phase
             int slot, j, st, r0, nt;
-            while (walk.next(slot, j, st, r0, nt)) {
+            for (int u = 0; walk.next(slot, j, st, r0, nt); ++u) {
                 const NarrowStage &cs = g.st[st];
+                if (g.trace) ntrace(g, u, NT_MMA_WAIT, globaltimer_ns());
                 if (st > 0 && r0 == 0) {
                     if (!mbar_wait(&bars->xready[slot], (uint32_t)(xr[slot] & 1), status,
                                    KERR_WAIT_FULL)) {
@@ -267,30 +289,35 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
                     ++xr[slot];
                     tc_fence_after();
                 }
-                const int nkb = (cs.K + G::BK - 1) / G::BK;
-                const uint32_t xb = smem_u32(xbuf + slot * G::X_BYTES);
-                for (int t = 0; t < nt; ++t, ++tiles) {
-                    const int acc = (int)(tiles % kNAcc);
-                    if (!mbar_wait(&bars->acc_empty[acc], ((tiles / kNAcc) & 1u) ^ 1u, status,
+                for (int t = 0; t < nt; ++t) {  // the unit's accumulators
+                    const unsigned tt = tiles + t;
+                    if (!mbar_wait(&bars->acc_empty[tt % kNAcc], ((tt / kNAcc) & 1u) ^ 1u, status,
                                    KERR_WAIT_ACC_EMPTY)) {
                         n_set_abort(bars);
                         goto mma_done;
                     }
+                }
+                tc_fence_after();
+                if (g.trace) ntrace(g, u, NT_MMA_START, globaltimer_ns());
+                const int nkb = (cs.K + G::BK - 1) / G::BK;
+                const uint32_t xb = smem_u32(xbuf + slot * g.x_bytes);
+                for (int kb = 0; kb < nkb; ++kb) {
+                    if (!mbar_wait(&bars->wfull[r], rph, status, KERR_WAIT_FULL)) {
+                        n_set_abort(bars);
+                        goto mma_done;
+                    }
                     tc_fence_after();
-                    const uint32_t d_tmem = tmem_base + acc * kNBN;
-                    for (int kb = 0; kb < nkb; ++kb) {
-                        if (!mbar_wait(&bars->wfull[r], rph, status, KERR_WAIT_FULL)) {
-                            n_set_abort(bars);
-                            goto mma_done;
-                        }
-                        tc_fence_after();
-                        const uint32_t a_addr = smem_u32(ring + r * G::SLOT_BYTES);
+                    const uint32_t s_addr = smem_u32(ring + r * g.slot_bytes);
+                    for (int t = 0; t < nt; ++t) {
+                        const uint32_t d_tmem = tmem_base + ((tiles + t) % kNAcc) * kNBN;
+                        const uint32_t a_addr = s_addr + t * kNABytes;
 #pragma unroll
                         for (int k = 0; k < 4; ++k) {
                             const uint64_t ad = smem_desc(a_addr + k * 32, 16, 1024, SMEM_SW128);
                             if (st == 0) {
-                                const uint64_t bd = smem_desc(a_addr + kNABytes + k * G::B_KSTEP,
-                                                              G::BOX_BYTES, 1024, SMEM_SW128);
+                                const uint64_t bd =
+                                    smem_desc(s_addr + g.ra * kNABytes + k * G::B_KSTEP,
+                                              G::BOX_BYTES, 1024, SMEM_SW128);
                                 tc_mma<KIND>(d_tmem, ad, bd, G::idesc_mn, (kb | k) != 0);
                             } else {
                                 const uint64_t bd =
@@ -298,14 +325,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
                                 tc_mma<KIND>(d_tmem, ad, bd, G::idesc_k, (kb | k) != 0);
                             }
                         }
-                        tc_commit(&bars->wempty[r]);
-                        if (++r == G::RING) {
-                            r = 0;
-                            rph ^= 1;
-                        }
                     }
-                    tc_commit(&bars->acc_full[acc]);
+                    tc_commit(&bars->wempty[r]);
+                    if (++r == RING) {
+                        r = 0;
+                        rph ^= 1;
+                    }
                 }
+                for (int t = 0; t < nt; ++t) tc_commit(&bars->acc_full[(tiles + t) % kNAcc]);
+                tiles += nt;
+                if (g.trace) ntrace(g, u, NT_MMA_END, globaltimer_ns());
                 if (n_aborted(bars)) break;
             }
         mma_done:
@@ -315,18 +344,27 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
     } else {
         // ------------------------------------------------------------ epilogues (warps 2..5)
         const int quarter = warp & 3;
-        const int et = threadIdx.x - 64;  // 0..127: this thread's column for the tail snapshot
-        uint8_t *staging = smem + G::STG_OFF + (warp - 2) * 2 * kStageBufBytes;
+        const int et = threadIdx.x - 64;  // 0..127: this thread's column for the tail quad
+        uint8_t *staging = stg0 + (warp - 2) * 2 * kStageBufBytes;
         int sbuf = 0;
         unsigned tiles = 0;
         uint32_t meet_ph = 0;
         bool ok = true;
         int slot, j, st, r0, nt;
-        while (ok && walk.next(slot, j, st, r0, nt)) {
+        for (int u = 0; ok && walk.next(slot, j, st, r0, nt); ++u) {
             const NarrowStage &cs = g.st[st];
             const bool last = st + 1 == g.n;
             const int n0 = walk.block_of(j) * kNBN;
-            uint8_t *xs = xbuf + slot * G::X_BYTES;
+            uint8_t *xs = xbuf + slot * g.x_bytes;
+            const bool tails = OP == OP_I8 && cs.tail_hi > cs.tail_lo;
+            // the first stage's input quad comes from global memory: load it
+            // before waiting for the accumulators, so the two latencies overlap
+            uint32_t qv0 = 0;
+            if (tails && st == 0 && n0 + et < g.N) {
+                const uint8_t *b = static_cast<const uint8_t *>(g.b);
+                for (int q = 0; q < 4 && q < cs.K; ++q)
+                    qv0 |= (uint32_t)b[(size_t)q * g.ldb + n0 + et] << (8 * q);
+            }
             // every tile of the unit: an intermediate overwrites the operand they read
             for (int t = 0; t < nt && ok; ++t) {
                 const unsigned tt = tiles + t;
@@ -335,18 +373,22 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
             }
             if (!ok) break;
             tc_fence_after();
-            // INT8 tail rows add weight quad 0 x input quad 0; a later stage's input
-            // quad is in this slot's operand buffer, copied aside before any warp
-            // overwrites it (every warp passes the meeting points alike)
-            const bool tails = OP == OP_I8 && cs.tail_hi > cs.tail_lo;
-            if (tails && st > 0) {
+            if (g.trace && quarter == 0 && lane == 0) ntrace(g, u, NT_EPI_START, globaltimer_ns());
+            // INT8 tail rows add weight quad 0 x input quad 0: the input's first
+            // four rows of this block's columns, copied aside first (a later stage's
+            // input is the operand buffer this unit overwrites); every warp passes
+            // the meeting points alike
+            if (tails) {
                 if (!(ok = epi_meet(bars, meet_ph, lane, status))) break;
-                quad[et] = *reinterpret_cast<const uint32_t *>(xs + kmaj<1>(0, et));
+                quad[et] = st > 0 ? *reinterpret_cast<const uint32_t *>(xs + kmaj<1>(0, et)) : qv0;
                 if (!(ok = epi_meet(bars, meet_ph, lane, status))) break;
             }
+            // rows of the next stage's operand that its MMAs read (k-blocks of BK)
+            const int xrows = (cs.M + G::BK - 1) / G::BK * G::BK;
             for (int t = 0; t < nt; ++t) {
                 const unsigned tt = tiles + t;
-                const int row = (r0 + t) * 128 + quarter * 32 + lane;  // stage output row
+                const int warp_row0 = (r0 + t) * 128 + quarter * 32;
+                const int row = warp_row0 + lane;  // stage output row
                 const uint32_t t_row =
                     tmem_base + (tt % kNAcc) * kNBN + ((uint32_t)(quarter * 32) << 16);
                 const bool tail_row = tails && row >= cs.tail_lo && row < cs.tail_hi;
@@ -354,9 +396,24 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
                 if (tail_row)
                     wq = *reinterpret_cast<const uint32_t *>(
                         cs.w_tail + (size_t)(row - cs.tail_row0) * cs.ld_w_tail + cs.K);
-                const int warp_row0 = (r0 + t) * 128 + quarter * 32;
+                // rows written: the result's stored rows; an INT8 intermediate's M
+                // rows (the next stage's weights are zero past its K = M, and
+                // 0 x anything is 0 in integers); a BF16 intermediate's rows up to
+                // the k-block end, zeros past M (a stale NaN x 0 would be NaN)
+                bool rows_out = warp_row0 < (last ? cs.out_rows : OP == OP_I8 ? cs.M : xrows);
+                if (OP == OP_BF16 && !last && rows_out && warp_row0 >= cs.M) {
+                    // a warp wholly past M: its 32 rows of every column are zero
+                    const int kb = warp_row0 / G::BK, c0 = (warp_row0 % G::BK) / 8;
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        const int idx = lane + 32 * i, n = idx >> 2, c = c0 + (idx & 3);
+                        *reinterpret_cast<uint4 *>(xs + kb * kNKbBytes + n * 128 + ((c ^ (n & 7)) << 4)) =
+                            make_uint4(0u, 0u, 0u, 0u);
+                    }
+                    rows_out = false;
+                }
 #pragma unroll 1
-                for (int c = 0; c < kNBN / 32; ++c) {
+                for (int c = 0; c < kNBN / 32 && rows_out; ++c) {
                     const int lc = c * 32, nc = n0 + lc;
                     if (nc >= g.N) break;  // warp-uniform
                     uint32_t v[32];
@@ -367,16 +424,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
                         for (int q = 0; q < 4; ++q) {
                             const int a = (int)((wq >> (8 * q)) & 0xffu);
 #pragma unroll
-                            for (int jj = 0; jj < 32; ++jj) {
-                                int x;
-                                if (st == 0)
-                                    x = nc + jj < g.N ? (int)reinterpret_cast<const int8_t *>(
-                                                            g.b)[(size_t)q * g.ldb + nc + jj]
-                                                      : 0;
-                                else
-                                    x = (int)(int8_t)((quad[lc + jj] >> (8 * q)) & 0xffu);
-                                v[jj] = (uint32_t)((int32_t)v[jj] + a * x);
-                            }
+                            for (int jj = 0; jj < 32; ++jj)
+                                v[jj] = (uint32_t)((int32_t)v[jj] +
+                                                   a * (int)(int8_t)((quad[lc + jj] >> (8 * q)) & 0xffu));
                         }
                     }
                     if (last) {
@@ -391,7 +441,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
                         sbuf ^= 1;
                         fence_proxy_async_smem();
                         __syncwarp();
-                        if (lane == 0 && warp_row0 < cs.out_rows) {
+                        if (lane == 0) {
                             tma_store_2d(&cs.tm_out, b0, nc, warp_row0);
                             bulk_commit();
                         }
@@ -422,7 +472,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
                             for (int u = 0; u < 8; ++u)
                                 *reinterpret_cast<uint32_t *>(xs + kmaj<1>(k0, lc + 8 * h + u)) =
                                     pack_s8x4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
-                        } else {
+                        } else if (row < cs.M) {
 #pragma unroll
                             for (int u = 0; u < 32; ++u)
                                 xs[kmaj<1>(row, lc + u)] = (uint8_t)(pack_s8x4(v[u], 0, 0, 0) & 0xffu);
@@ -434,6 +484,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
                 if (lane == 0) mbar_arrive(&bars->acc_empty[tt % kNAcc]);
             }
             tiles += nt;
+            if (g.trace && quarter == 0 && lane == 0) ntrace(g, u, NT_EPI_END, globaltimer_ns());
             if (!last) {
                 // the next stage's input is in place: tell the MMA warp
                 fence_proxy_async_smem();
@@ -473,30 +524,48 @@ bool narrow_eligible(const StageArgs *st, int n)
 
 namespace {
 
+// The shared memory layout of a chain: the weight boxes of the widest unit
+// (row tiles of the widest intermediate) and the first stage's activations per
+// ring slot; operand buffers as deep as the widest intermediate; two column
+// blocks in flight when that leaves at least three ring slots, else one.
 template <int OP>
-cudaError_t narrow_capacity(int &per_sm)
+bool narrow_layout(const StageArgs *st, int n, NarrowArgs &A)
 {
     using G = NarrowGeo<OP>;
+    int ra = 1, xkb = 1;
+    for (int i = 0; i + 1 < n; ++i) {
+        ra = std::max(ra, (st[i].M + 127) / 128);
+        xkb = std::max(xkb, (st[i].M + G::BK - 1) / G::BK);
+    }
+    A.ra = ra;
+    A.slot_bytes = ra * kNABytes + G::B_BYTES;
+    A.x_bytes = xkb * kNKbBytes;
+    for (int xs = 2; xs >= 1; --xs) {
+        const int avail = kNMaxSmem - kNFixedBytes - xs * A.x_bytes;
+        const int ring = std::min(kNarrowMaxRing, avail / A.slot_bytes);
+        if (ring >= (xs == 2 ? 3 : 2)) {
+            A.ring = ring;
+            A.xslots = xs;
+            A.smem = ring * A.slot_bytes + xs * A.x_bytes + kNFixedBytes;
+            return true;
+        }
+    }
+    return false;
+}
+
+template <int OP>
+cudaError_t narrow_attr(int smem)
+{
     static std::mutex mu;
-    static unsigned long long known = 0;
-    static int cap[64];
+    static int done[64];
     std::lock_guard<std::mutex> lk(mu);
     int dev = 0;
     cudaGetDevice(&dev);
-    if (!(known & (1ull << (dev & 63)))) {
-        cudaError_t e = cudaFuncSetAttribute(tc_narrow_kernel<OP>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-        if (e != cudaSuccess) return e;
-        int n = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tc_narrow_kernel<OP>, kThreads, G::SMEM);
-        if (e != cudaSuccess || n < 1) {
-            cudaGetLastError();
-            return cudaErrorNotSupported;
-        }
-        cap[dev & 63] = n;
-        known |= 1ull << (dev & 63);
-    }
-    per_sm = cap[dev & 63];
+    if (done[dev & 63] >= smem) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(tc_narrow_kernel<OP>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, kNMaxSmem);
+    if (e != cudaSuccess) return e;
+    done[dev & 63] = kNMaxSmem;
     return cudaSuccess;
 }
 
@@ -561,6 +630,7 @@ cudaError_t plan_narrow_op(const StageArgs *st, int n, int num_sms, NarrowArgs &
             if (i + 1 == n && !make_out_map(&cs.tm_out, a)) return cudaErrorNotSupported;
             if (i + 1 < n) cs.tm_out = cs.tm_w;
         }
+        if (!narrow_layout<OP>(st, n, A)) return cudaErrorNotSupported;
         A.b = st[0].x;
         A.ldb = st[0].ld_x;
         A.op = OP;
@@ -575,11 +645,10 @@ cudaError_t plan_narrow_op(const StageArgs *st, int n, int num_sms, NarrowArgs &
         built.push_back(b.release());
         P = &built.back()->P;
     }
-    int per_sm = 0;
-    cudaError_t e = narrow_capacity<OP>(per_sm);
+    const cudaError_t e = narrow_attr<OP>(P->smem);
     if (e != cudaSuccess) return e;
     out = *P;  // a copy: the cache may drop this entry once the lock is released
-    grid = std::min(P->nblocks, per_sm * num_sms);
+    grid = std::min(P->nblocks, num_sms);  // one CTA per SM (shared memory)
     return cudaSuccess;
 }
 
@@ -592,13 +661,19 @@ cudaError_t plan_narrow(const StageArgs *st, int n, int num_sms, NarrowArgs &out
                                : plan_narrow_op<OP_I8>(st, n, num_sms, out, grid);
 }
 
+int narrow_units_per_cta(const NarrowArgs &P, int grid)
+{
+    const int per_block = P.n - 1 + (P.st[P.n - 1].M + 127) / 128;
+    return (P.nblocks + grid - 1) / grid * per_block;
+}
+
 cudaError_t launch_narrow(NarrowArgs &P, int grid, int *status, cudaStream_t s)
 {
     P.status = status;
     if (P.op == OP_BF16)
-        tc_narrow_kernel<OP_BF16><<<grid, kThreads, NarrowGeo<OP_BF16>::SMEM, s>>>(P);
+        tc_narrow_kernel<OP_BF16><<<grid, kThreads, P.smem, s>>>(P);
     else
-        tc_narrow_kernel<OP_I8><<<grid, kThreads, NarrowGeo<OP_I8>::SMEM, s>>>(P);
+        tc_narrow_kernel<OP_I8><<<grid, kThreads, P.smem, s>>>(P);
     return cudaGetLastError();
 }
 

@@ -34,11 +34,30 @@ __device__ __forceinline__ uint64_t wait_limit_ns()
     return *reinterpret_cast<volatile unsigned long long *>(&fg_wait_limit_ns);
 }
 
+// Every wait limit the host may set is at least this long (fg_selftest_timeout
+// takes 100 us and more), so a wait reads the limit only once it has lasted
+// this long: the waits of a healthy run end sooner and never load it.
+constexpr uint64_t kWaitQuietNs = 50000;
+
 __device__ __forceinline__ uint64_t globaltimer_ns()
 {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
+}
+
+// True once a wait that began at t0 has run past the limit.
+__device__ __forceinline__ bool wait_expired(uint64_t t0)
+{
+    const uint64_t el = globaltimer_ns() - t0;
+    return el > kWaitQuietNs && el > wait_limit_ns();
+}
+
+__device__ __forceinline__ uint32_t smid()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
+    return r;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -95,10 +114,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *s
     const uint32_t a = smem_u32(bar);
     if (mbar_try_wait(a, parity)) return true;
     const uint64_t t0 = globaltimer_ns();
-    const uint64_t limit = wait_limit_ns();
     while (true) {
         if (mbar_try_wait(a, parity)) return true;
-        if (globaltimer_ns() - t0 > limit) {
+        if (wait_expired(t0)) {
             atomicCAS(status, 0, code);
             return false;
         }
