@@ -119,6 +119,20 @@ def get_chain_mode():
     return lib().fg_get_chain_mode()
 
 
+FG_NARROW_OFF, FG_NARROW_ALWAYS, FG_NARROW_AUTO = 0, 1, 2
+
+
+def set_narrow(mode):
+    """When fused BF16 / INT8 chains keep narrow intermediates on chip:
+    "auto" (where measured faster), "always" or "off" (fg_set_narrow)."""
+    lib().fg_set_narrow({"off": FG_NARROW_OFF, "always": FG_NARROW_ALWAYS,
+                         "auto": FG_NARROW_AUTO}.get(mode, mode))
+
+
+def get_narrow():
+    return {FG_NARROW_OFF: "off", FG_NARROW_ALWAYS: "always", FG_NARROW_AUTO: "auto"}[lib().fg_get_narrow()]
+
+
 def sync():
     st = lib().fg_sync()
     if st != FG_OK:

@@ -329,20 +329,26 @@ bool fused_enabled()
 }
 bool g_fused_unsupported[64];
 
-// Chains whose intermediates fit on chip (FG_NARROW=0: never).
-bool narrow_enabled()
+// Chains whose intermediates fit on chip: FG_NARROW_AUTO (default), _ALWAYS
+// or _OFF; the environment variable FG_NARROW (0 / 1) sets the initial mode.
+std::atomic<int> g_narrow_mode{-1};
+int narrow_mode()
 {
-    static const bool on = [] {
+    int m = g_narrow_mode.load();
+    if (m < 0) {
         const char *v = getenv("FG_NARROW");
-        return !(v && v[0] == '0');
-    }();
-    return on;
+        m = v && v[0] == '0' ? FG_NARROW_OFF : v && v[0] == '1' ? FG_NARROW_ALWAYS : FG_NARROW_AUTO;
+        g_narrow_mode.store(m);
+    }
+    return m;
 }
 
 int launch_stages(DevCtx *c, int kind, std::vector<StageArgs> &stages, long N)
 {
     const int n = (int)stages.size();
-    if (fused_enabled() && narrow_enabled() && narrow_eligible(stages.data(), n)) {
+    const int nm = fused_enabled() ? narrow_mode() : FG_NARROW_OFF;
+    if (nm != FG_NARROW_OFF && narrow_eligible(stages.data(), n) &&
+        (nm == FG_NARROW_ALWAYS || narrow_preferred(stages.data(), n, c->sms))) {
         // intermediates on chip; a chain whose operands the tensor maps cannot
         // describe (unaligned rows) falls through to the fused chain
         static thread_local NarrowArgs P;
@@ -1410,6 +1416,11 @@ FG_EXPORT void fg_set_chain_mode(int mode)
 {
     g_chain_mode.store(mode == FG_CHAIN_PER_GEMM ? FG_CHAIN_PER_GEMM : FG_CHAIN_FUSED);
 }
+FG_EXPORT void fg_set_narrow(int mode)
+{
+    g_narrow_mode.store(mode == FG_NARROW_OFF || mode == FG_NARROW_ALWAYS ? mode : FG_NARROW_AUTO);
+}
+FG_EXPORT int fg_get_narrow(void) { return narrow_mode(); }
 FG_EXPORT int fg_get_chain_mode(void) { return fused_enabled() ? FG_CHAIN_FUSED : FG_CHAIN_PER_GEMM; }
 FG_EXPORT unsigned long long fg_kernel_launches(void) { return g_launches.load(); }
 FG_EXPORT const char *fg_version(void) { return "flashgemm-b200 0.1 (sm_100a)"; }

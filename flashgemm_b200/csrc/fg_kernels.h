@@ -207,6 +207,8 @@ struct alignas(64) NarrowArgs {
 constexpr int kNarrowTraceFields = 8;
 
 bool narrow_eligible(const StageArgs *st, int n);
+// Where the narrow kernel is measured faster than the fused chain kernel.
+bool narrow_preferred(const StageArgs *st, int n, int num_sms);
 // The launch parameters and grid of a chain's narrow launch (tensor maps kept
 // for the last few operand sets); cudaErrorNotSupported when it does not qualify.
 cudaError_t plan_narrow(const StageArgs *st, int n, int num_sms, NarrowArgs &out, int &grid);

@@ -522,6 +522,19 @@ bool narrow_eligible(const StageArgs *st, int n)
     return true;
 }
 
+// On B200, over the reference's chain table (N 3136..65536, K_1 288..4800):
+// INT8 chains run faster narrow at every width (their fused path pays the
+// tail-row preparation and an int8 round trip per stage); BF16 chains whose
+// 128-column blocks fill fewer than half the SMs run their deep first stage on
+// too few SMs and are faster on the fused chain kernel, which splits rows too.
+bool narrow_preferred(const StageArgs *st, int n, int num_sms)
+{
+    (void)n;
+    if (st[0].op == OP_I8) return true;
+    const long nblk = (st[0].N + kNBN - 1) / kNBN;
+    return 2 * nblk >= num_sms;
+}
+
 namespace {
 
 // The shared memory layout of a chain: the weight boxes of the widest unit

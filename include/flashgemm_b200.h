@@ -73,6 +73,18 @@ enum { FG_CHAIN_FUSED = 0, FG_CHAIN_PER_GEMM = 1 };
 void fg_set_chain_mode(int mode);
 int fg_get_chain_mode(void);
 
+/* Fused BF16 / INT8 chains whose intermediates have at most 256 rows can keep
+ * them on chip (the narrow chain kernel: one CTA per 128-column block, each
+ * intermediate narrowed and permuted straight into shared memory; same
+ * results as the other paths).
+ * FG_NARROW_AUTO (default): where it is measured faster: every INT8 chain, and
+ *   BF16 chains with at least one 128-column block per two SMs.
+ * FG_NARROW_ALWAYS: every such chain.  FG_NARROW_OFF: never.
+ * The environment variable FG_NARROW (0 / 1 / auto) sets the initial mode. */
+enum { FG_NARROW_OFF = 0, FG_NARROW_ALWAYS = 1, FG_NARROW_AUTO = 2 };
+void fg_set_narrow(int mode);
+int fg_get_narrow(void);
+
 /* Element types of a chain. */
 enum { FG_DT_F32 = 0, FG_DT_BF16 = 1, FG_DT_INT8 = 2 };
 

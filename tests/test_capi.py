@@ -99,6 +99,11 @@ def test_settings_round_trip(fg):
     fg.set_semantics("ref")
     assert fg.get_semantics() == fg.FG_SEM_REF
     assert "sm_100a" in fg.version()
+    for mode in ("off", "always", "auto"):
+        fg.set_narrow(mode)
+        assert fg.get_narrow() == mode
+    fg.set_narrow(7)  # anything else: the measured default
+    assert fg.get_narrow() == "auto"
 
 
 def test_group_config_round_trip(fg):
