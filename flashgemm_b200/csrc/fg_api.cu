@@ -296,6 +296,8 @@ size_t chain_scratch(int dtype, int algo, long N, int n, const long *M, const lo
             if (K[i] % 8) s += carve_size((size_t)M[i] * round_up(K[i], 8) * 2);
         s += 2 * carve_size((size_t)maxM * ldN * 2);
     } else if (algo == FG_F32_3XTF32) {
+        if (getenv("FG_TRACE_DIR"))  // per-tile timeline of the panel-resident kernel
+            s += carve_size((size_t)((N + 127) / 128) * kPanelMaxStages * kPanelTraceFields * 8);
         for (int i = 0; i < n; ++i) s += 2 * carve_size((size_t)M[i] * round_up(K[i], 4) * 4);
         s += 2 * carve_size((size_t)K[0] * ldN * 4);                 // split input
         s += 2 * 2 * carve_size((size_t)maxM * ldN * 4);             // ping-pong hi/lo
@@ -706,9 +708,40 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
                                      cudaMemcpyHostToDevice, c->work));
             CUDA_TRY(cudaMemcpyAsync(od, gx.panel_off.data(), gx.panel_off.size() * sizeof(int),
                                      cudaMemcpyHostToDevice, c->work));
-            return run_kernel(c, FG_PK_TC_TF32X3, fl, "panel-resident chain", [&] {
-                return launch_panel(pd, bd, od, gx.panel_ctas, c->status, c->work);
+            // FG_TRACE_DIR=<dir>: a per-tile timeline of every panel launch
+            static const char *trace_dir = getenv("FG_TRACE_DIR");
+            const size_t trace_words = gx.panel_blocks.size() * kPanelMaxStages * kPanelTraceFields;
+            unsigned long long *trace = nullptr;
+            if (trace_dir) {
+                trace = (unsigned long long *)arena_take(c, trace_words * 8);
+                CUDA_TRY(cudaMemsetAsync(trace, 0, trace_words * 8, c->work));
+            }
+            st = run_kernel(c, FG_PK_TC_TF32X3, fl, "panel-resident chain", [&] {
+                return launch_panel(pd, bd, od, gx.panel_ctas, c->status, c->work, trace);
             });
+            if (st == FG_OK && trace) {
+                std::vector<unsigned long long> h(trace_words);
+                CUDA_TRY(cudaMemcpyAsync(h.data(), trace, trace_words * 8, cudaMemcpyDeviceToHost,
+                                         c->work));
+                CUDA_TRY(cudaStreamSynchronize(c->work));
+                static int seq = 0;
+                char path[1024];
+                snprintf(path, sizeof path, "%s/panel_trace_%d.csv", trace_dir, seq++);
+                if (FILE *f = fopen(path, "w")) {
+                    fprintf(f, "pos,stage,slot,sm,cta,prod_start,prod_end,mma_wait,mma_start,mma_end,"
+                               "epi_start,epi_end,split_start,split_end\n");
+                    for (size_t r = 0; r < trace_words / kPanelTraceFields; ++r) {
+                        const unsigned long long *v = &h[r * kPanelTraceFields];
+                        if (!v[1]) continue;  // no such tile
+                        fprintf(f, "%zu,%zu,%llu,%llu,%llu", r / kPanelMaxStages, r % kPanelMaxStages,
+                                v[0] & 0xff, (v[0] >> 16) & 0xffff, v[0] >> 32);
+                        for (int k = 1; k < kPanelTraceFields; ++k) fprintf(f, ",%llu", v[k]);
+                        fprintf(f, "\n");
+                    }
+                    fclose(f);
+                }
+            }
+            return st;
         }
         float *xh = (float *)arena_take(c, (size_t)K[0] * ldN * 4);
         float *xl = (float *)arena_take(c, (size_t)K[0] * ldN * 4);

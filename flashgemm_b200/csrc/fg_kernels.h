@@ -228,8 +228,9 @@ constexpr int kPanelMaxStages = 8;
 // One chain's device descriptor (tensor maps and shapes).
 struct alignas(64) PanelChain {
     CUtensorMap tm_b;                        // B: K[0] x N FP32, MN-major boxes
-    CUtensorMap tm_c;                        // C: M_last x N FP32 (staged TMA stores)
-    CUtensorMap tm_w[kPanelMaxStages][2];    // weights (hi, lo), K-major boxes of 128 rows
+    CUtensorMap tm_w[kPanelMaxStages][2];    // weights (hi, lo), K-major boxes of 64 rows
+    float *C;                                // M_last x N FP32, row stride ldc
+    long ldc;
     int n;                                   // stages
     int N;
     int K[kPanelMaxStages + 1];              // K[i]: stage i's depth; K[i + 1] = M_i
@@ -242,7 +243,11 @@ struct PanelArgs {
     const uint32_t *blocks;
     const int *off;
     int *status;
+    // optional (else null): kPanelTraceFields %globaltimer stamps per
+    // (block position, stage), rows at (position * kPanelMaxStages + stage)
+    unsigned long long *trace;
 };
+constexpr int kPanelTraceFields = 10;
 
 // Host description of one chain for panel_chain_desc (device pointers).
 struct PanelChainArgs {
@@ -266,7 +271,8 @@ void panel_plan(const std::vector<int> &stage_kb, const std::vector<int> &nblock
                 std::vector<uint32_t> &blocks, std::vector<int> &off);
 cudaError_t panel_capacity(int num_sms, int &ctas);
 cudaError_t launch_panel(const PanelChain *chains_dev, const uint32_t *blocks_dev, const int *off_dev,
-                         int ctas, int *status, cudaStream_t s);
+                         int ctas, int *status, cudaStream_t s,
+                         unsigned long long *trace = nullptr);
 
 // Plain FP32 SGEMM on CUDA cores: C = A * B, one FMA per k in increasing k;
 // with kblock > 0 each block of kblock k is summed from zero and added to C.

@@ -7,24 +7,31 @@
 // kernel does the same on a B200 SM for chains whose dimensions are all at most
 // kPanelKMax (the tall-skinny chains: N up to 65536 columns, 64 x 64 weights):
 // a CTA loads a 128-column block of B once (TMA), splits it in place in shared
-// memory into the TF32 (hi, lo) pair, and runs every stage on the tensor cores;
-// the epilogue of stage i splits its FP32 result into stage i + 1's (hi, lo)
-// operand and writes it K-major into shared memory, where stage i + 1's MMAs
-// read it. Only the last stage's result goes to global memory. Weights (a few
-// KB per stage) stream from L2 through a two-slot TMA ring.
+// memory into the TF32 (hi, lo) pair, and runs every stage on the tensor cores.
 //
-// The arithmetic is the grouped 3xTF32 kernel's (fg_group.cu), operation for
-// operation: per 32-deep k-block four K = 8 MMAs, each the correction terms
-// hi*lo then lo*hi into their own accumulator and hi*hi into the partial sum;
-// the partial sum handed to FP32 registers every `kchunk` k-blocks and summed in
-// order, the correction added once; the same round-to-nearest TF32 split. The
-// results are bit-identical to that kernel's.
+// Each stage computes the transposed product, D^T = X^T W^T: the block's 128
+// columns are the MMA's M (every TMEM lane holds a column, so all four lane
+// quarters carry data) and the stage's at most 64 output rows its N. An
+// epilogue thread so owns one column and all its output rows: for an
+// intermediate it writes that column's (hi, lo) values as one K-major row of
+// the next stage's A operand (16-byte stores into shared memory); for the last
+// stage it stores them to global memory, each warp writing 32 consecutive
+// columns of an output row at a time. Weights (a few KB per stage) stream from
+// L2 through a TMA ring as the B operand.
+//
+// The arithmetic is the grouped 3xTF32 kernel's (fg_group.cu) with the operand
+// roles exchanged: per 32-deep k-block four K = 8 MMAs, each the correction
+// terms lo*hi then hi*lo into their own accumulator and hi*hi into the partial
+// sum; the partial sum handed to FP32 registers every `kchunk` k-blocks and
+// summed in order, the correction added once; the same round-to-nearest TF32
+// split.
 //
 // Two column blocks are in flight per CTA (two operand buffers), their tiles
 // interleaved (block A stage 0, block B stage 0, A 1, B 1, ...), so that one
 // block's MMAs run while the other's epilogue drains. Warp 0 is the TMA
-// producer, warp 1 allocates TMEM and issues MMAs, warps 2-5 split stage-0
-// inputs and run the epilogues. Every wait is bounded (fg_ptx.cuh).
+// producer, warp 1 allocates TMEM and issues MMAs, warps 2-9 split stage-0
+// inputs and run the epilogues (two warps per TMEM lane quarter, 32 output
+// rows each). Every wait is bounded (fg_ptx.cuh).
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -39,7 +46,7 @@ namespace fg {
 
 namespace {
 
-constexpr int kPBN = 128;                      // columns per block (MMA N)
+constexpr int kPBN = 128;                      // columns per block (MMA M)
 constexpr int kPBK = 32;                       // TF32 elements per 128-byte k-block
 constexpr int kPKb = kPanelKMax / kPBK;        // k-blocks of the largest operand
 constexpr int kPBoxN = 32;                     // MN-major box: 32 columns (128 bytes)
@@ -47,93 +54,101 @@ constexpr int kPBoxBytes = kPBoxN * kPBK * 4;  // 4 KB
 constexpr int kPKbBytes = kPBN * kPBK * 4;     // one k-block of a (hi or lo) operand: 16 KB
 constexpr int kPPartBytes = kPKb * kPKbBytes;  // hi or lo of one block: 32 KB
 constexpr int kPSlotBytes = 2 * kPPartBytes;   // (hi, lo) of one block in flight
-constexpr int kPWBytes = 128 * 128;            // one k-block of weights (128 rows x 128 B)
-constexpr int kPRing = 2;                      // weight ring slots, each (hi, lo)
+constexpr int kPRowsN = kPanelKMax;            // MMA N: output rows of a stage (padded)
+constexpr int kPWBytes = kPRowsN * 128;        // one k-block of weights: 64 rows x 128 B
+constexpr int kPRing = 6;                      // weight ring slots, each (hi, lo)
+constexpr int kPEpiWarps = 8;                  // two per TMEM lane quarter, 32 rows each
+constexpr int kPThreads = 64 + 32 * kPEpiWarps;
 constexpr int kPXOff = 0;
 constexpr int kPWOff = kPXOff + 2 * kPSlotBytes;
-constexpr int kPStageOff = kPWOff + kPRing * 2 * kPWBytes;
-constexpr int kPBarOff = kPStageOff + kEpiStagingBytes;
-constexpr int kPSmem = kPBarOff + 256 + 1024;  // + barriers + alignment slack
-constexpr int kPTmemCols = 4 * kPBN;           // 2 partial-sum + 2 correction accumulators
+constexpr int kPBarOff = kPWOff + kPRing * 2 * kPWBytes;
+constexpr int kPSmem = kPBarOff + 512 + 1024;  // + barriers + alignment slack
+constexpr int kPAcc = 4;                       // partial-sum accumulators (one per FP32 chunk)
+constexpr int kPCorr = 4;                      // correction accumulators (one per tile)
+constexpr int kPTmemCols = (kPAcc + kPCorr) * kPRowsN;
 static_assert(kPSmem <= 232448, "shared memory per CTA");
-static_assert(kPTmemCols <= 512, "TMEM columns");
+static_assert(kPTmemCols == 512, "TMEM allocation: a power of two");
 
-// D F32, A TF32, B TF32, A K-major; B MN-major (stage 0, as TMA lands it) or
-// K-major (later stages, as the epilogue writes it)
-constexpr uint32_t kIdescMN = make_idesc(1, 2, 2, 0, 1, kBM, kPBN);
-constexpr uint32_t kIdescK = make_idesc(1, 2, 2, 0, 0, kBM, kPBN);
+// D F32, A TF32 (the activations: MN-major for stage 0, as TMA lands them,
+// K-major for later stages, as the epilogue writes them), B TF32 (the weights,
+// K-major); M = 128 columns, N = 64 output rows
+constexpr uint32_t kIdescMN = make_idesc(1, 2, 2, 1, 0, kPBN, kPRowsN);
+constexpr uint32_t kIdescK = make_idesc(1, 2, 2, 0, 0, kPBN, kPRowsN);
 
 struct __align__(8) PanelBars {
     uint64_t wfull[kPRing], wempty[kPRing];   // weight ring
     uint64_t xin[2];      // stage-0 input of a block landed in its operand buffer (TMA bytes)
-    uint64_t xready[2];   // the operand buffer holds the next tile's B (4 epilogue warps)
+    uint64_t xready[2];   // the operand buffer holds the next tile's A (kPEpiWarps arrivals)
     uint64_t xfree[2];    // the MMAs of a block's last stage are done: the buffer may refill
-    uint64_t acc_full[2], acc_empty[2];    // partial-sum accumulators
-    uint64_t corr_full[2], corr_empty[2];  // correction accumulators
+    uint64_t acc_full[kPAcc], acc_empty[kPAcc];      // partial-sum accumulators
+    uint64_t corr_full[kPCorr], corr_empty[kPCorr];  // correction accumulators
     uint64_t mma_done;
     uint32_t tmem_base;
     int abort;
 };
-static_assert(sizeof(PanelBars) <= 256, "barrier block");
+static_assert(sizeof(PanelBars) <= 512, "barrier block");
 
 __device__ __forceinline__ void p_set_abort(PanelBars *b) { *reinterpret_cast<volatile int *>(&b->abort) = 1; }
 __device__ __forceinline__ bool p_aborted(PanelBars *b) { return *reinterpret_cast<volatile int *>(&b->abort) != 0; }
 
 // The tiles of one CTA in the order every role walks them: the CTA's blocks
 // alternate between operand buffers (slot = position % 2), and the tiles of
-// the two slots' current blocks interleave, one tile of each in turn.
+// the two slots' current blocks interleave, one tile of each in turn. (Plain
+// fields rather than arrays, so the walk stays in registers.)
 struct TileWalk {
     const PanelArgs *g;
-    int q0, q1;   // this CTA's blocks: g->blocks[q0 .. q1)
-    int pos[2];   // slot s: position (q0 + s, q0 + s + 2, ...) of its current block
-    int stage[2];
+    int q0, q1;          // this CTA's blocks: g->blocks[q0 .. q1)
+    int pos0, pos1;      // slot s: position (q0 + s, q0 + s + 2, ...) of its current block
+    int stage0, stage1;
     int turn;
     __device__ void init(const PanelArgs &args, int cta)
     {
         g = &args;
         q0 = args.off[cta];
         q1 = args.off[cta + 1];
-        pos[0] = q0;
-        pos[1] = q0 + 1;
-        stage[0] = stage[1] = 0;
+        pos0 = q0;
+        pos1 = q0 + 1;
+        stage0 = stage1 = 0;
         turn = 0;
     }
     __device__ int stages_of(int q) const { return g->chains[g->blocks[q] >> 16].n; }
     // Next tile: slot, block position, stage, whether it is the block's last
-    // stage, and the next block position of that slot (q1 and beyond: none).
-    // false when the CTA has no more tiles.
+    // stage. false when the CTA has no more tiles.
     __device__ bool next(int &slot, int &q, int &st, bool &last)
     {
         int s = turn;
-        if (pos[s] >= q1) s ^= 1;
-        if (pos[s] >= q1) return false;
+        if ((s ? pos1 : pos0) >= q1) s ^= 1;
+        const int p = s ? pos1 : pos0;
+        if (p >= q1) return false;
         slot = s;
-        q = pos[s];
-        st = stage[s];
+        q = p;
+        st = s ? stage1 : stage0;
         last = st + 1 == stages_of(q);
-        if (last) {
-            pos[s] += 2;
-            stage[s] = 0;
+        const int np = last ? p + 2 : p;
+        const int ns = last ? 0 : st + 1;
+        if (s) {
+            pos1 = np;
+            stage1 = ns;
         } else {
-            ++stage[s];
+            pos0 = np;
+            stage0 = ns;
         }
         turn = s ^ 1;
         return true;
     }
 };
 
-// K-major (hi or lo) operand: element (k, n) of a block, 128-byte rows of 32
-// k-values per column n, 16-byte chunks swizzled over 8-row atoms (the layout
-// a TMA load with 128-byte swizzle gives a K-major operand).
-__device__ __forceinline__ uint32_t kmajor_off(int k, int n)
+// Timeline of a tile (FG_TRACE_DIR): its description, then the roles' stamps.
+enum { PT_DESC, PT_PROD_START, PT_PROD_END, PT_MMA_WAIT, PT_MMA_START, PT_MMA_END, PT_EPI_START,
+       PT_EPI_END, PT_SPLIT_START, PT_SPLIT_END };
+__device__ __forceinline__ void ptrace(const PanelArgs &g, int q, int st, int f, unsigned long long v)
 {
-    const int kk = k & 31;
-    return (uint32_t)((k >> 5) * kPKbBytes + n * 128 + ((((kk >> 2) ^ (n & 7)) << 4)) + (kk & 3) * 4);
+    g.trace[((size_t)q * kPanelMaxStages + st) * kPanelTraceFields + f] = v;
 }
 
 }  // namespace
 
-__global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_constant__ PanelArgs g)
+__global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_constant__ PanelArgs g)
 {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
@@ -152,12 +167,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
         }
         for (int s = 0; s < 2; ++s) {
             mbar_init(&bars->xin[s], 1);
-            mbar_init(&bars->xready[s], 4);
+            mbar_init(&bars->xready[s], kPEpiWarps);
             mbar_init(&bars->xfree[s], 1);
-            mbar_init(&bars->acc_full[s], 1);
-            mbar_init(&bars->acc_empty[s], 4);
-            mbar_init(&bars->corr_full[s], 1);
-            mbar_init(&bars->corr_empty[s], 4);
+        }
+        for (int a = 0; a < kPAcc; ++a) {
+            mbar_init(&bars->acc_full[a], 1);
+            mbar_init(&bars->acc_empty[a], kPEpiWarps);
+        }
+        for (int a = 0; a < kPCorr; ++a) {
+            mbar_init(&bars->corr_full[a], 1);
+            mbar_init(&bars->corr_empty[a], kPEpiWarps);
         }
         mbar_init(&bars->mma_done, 1);
         bars->abort = 0;
@@ -179,23 +198,36 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
             uint32_t rph = 0;
             uint32_t pending = 0, pending_ph = 0;  // ring slots with loads in flight
             uint32_t xin_pending = 0;              // operand buffers with a load in flight
-            uint32_t xin_ph[2] = {0, 0};
-            int loaded[2] = {0, 0};                // blocks loaded into each buffer so far
+            uint32_t xin_ph0 = 0, xin_ph1 = 0;
+            int loaded0 = 0, loaded1 = 0;          // blocks loaded into each buffer so far
             int slot, q, st;
             bool last;
             while (walk.next(slot, q, st, last)) {
                 const uint32_t bq = g.blocks[q];
                 const PanelChain &ch = g.chains[bq >> 16];
                 const int n0 = (int)(bq & 0xffffu) * kPBN;
+                if (g.trace) {
+                    ptrace(g, q, st, PT_DESC,
+                           (unsigned long long)slot | (unsigned long long)st << 8 |
+                               (unsigned long long)smid() << 16 | (unsigned long long)blockIdx.x << 32);
+                    ptrace(g, q, st, PT_PROD_START, globaltimer_ns());
+                }
                 if (st == 0) {
                     // this block's B into the slot's buffer once the slot's previous
                     // block's last MMAs are done
-                    if (!mbar_wait(&bars->xfree[slot], (uint32_t)(loaded[slot] & 1) ^ 1u, status,
+                    const int loaded = slot ? loaded1 : loaded0;
+                    if (!mbar_wait(&bars->xfree[slot], (uint32_t)(loaded & 1) ^ 1u, status,
                                    KERR_WAIT_EMPTY)) {
                         p_set_abort(bars);
                         goto producer_done;
                     }
-                    ++loaded[slot];
+                    if (slot) {
+                        ++loaded1;
+                        xin_ph1 = (uint32_t)(loaded & 1);
+                    } else {
+                        ++loaded0;
+                        xin_ph0 = (uint32_t)(loaded & 1);
+                    }
                     const int nkb = (ch.K[0] + kPBK - 1) / kPBK;
                     int nvb = (ch.N - n0 + kPBoxN - 1) / kPBoxN;  // boxes that start inside N
                     nvb = nvb < kPBN / kPBoxN ? nvb : kPBN / kPBoxN;
@@ -206,7 +238,6 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
                             tma_load_2d(x + kb * kPKbBytes + j * kPBoxBytes, &ch.tm_b, &bars->xin[slot],
                                         n0 + j * kPBoxN, kb * kPBK);
                     xin_pending |= 1u << slot;
-                    xin_ph[slot] = (uint32_t)((loaded[slot] - 1) & 1);
                 }
                 const int nkb = (ch.K[st] + kPBK - 1) / kPBK;
                 for (int kb = 0; kb < nkb; ++kb) {
@@ -225,6 +256,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
                         rph ^= 1;
                     }
                 }
+                if (g.trace) ptrace(g, q, st, PT_PROD_END, globaltimer_ns());
                 if (p_aborted(bars)) break;
             }
         producer_done:
@@ -232,8 +264,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
             for (int i = 0; i < kPRing; ++i)
                 if (pending & (1u << i))
                     mbar_wait(&bars->wfull[i], (pending_ph >> i) & 1u, status, KERR_WAIT_FULL);
-            for (int s = 0; s < 2; ++s)
-                if (xin_pending & (1u << s)) mbar_wait(&bars->xin[s], xin_ph[s], status, KERR_WAIT_FULL);
+            if (xin_pending & 1u) mbar_wait(&bars->xin[0], xin_ph0, status, KERR_WAIT_FULL);
+            if (xin_pending & 2u) mbar_wait(&bars->xin[1], xin_ph1, status, KERR_WAIT_FULL);
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
@@ -242,17 +274,17 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
             uint32_t rph = 0;
             int acc = 0, cb = 0;
             uint32_t acc_ph = 0, cb_ph = 0;
-            int tiles[2] = {0, 0};  // tiles issued per slot: the xready phase to wait for
+            int tiles0 = 0, tiles1 = 0;  // tiles issued per slot: the xready phase to wait for
             int slot, q, st;
             bool last;
             while (walk.next(slot, q, st, last)) {
                 const PanelChain &ch = g.chains[g.blocks[q] >> 16];
-                if (!mbar_wait(&bars->xready[slot], (uint32_t)(tiles[slot] & 1), status,
-                               KERR_WAIT_FULL)) {
+                if (g.trace) ptrace(g, q, st, PT_MMA_WAIT, globaltimer_ns());
+                const int tiles = slot ? tiles1++ : tiles0++;
+                if (!mbar_wait(&bars->xready[slot], (uint32_t)(tiles & 1), status, KERR_WAIT_FULL)) {
                     p_set_abort(bars);
                     goto mma_done;
                 }
-                ++tiles[slot];
                 tc_fence_after();
                 const int num_kb = (ch.K[st] + kPBK - 1) / kPBK;
                 const int kchunk = ch.kchunk[st] > 0 ? ch.kchunk[st] : num_kb;
@@ -261,7 +293,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
                     goto mma_done;
                 }
                 tc_fence_after();
-                const uint32_t c_tmem = tmem_base + 2 * kPBN + cb * kPBN;
+                if (g.trace) ptrace(g, q, st, PT_MMA_START, globaltimer_ns());
+                const uint32_t c_tmem = tmem_base + (kPAcc + cb) * kPRowsN;
                 const uint32_t x_hi = smem_u32(xbuf + slot * kPSlotBytes);
                 const uint32_t x_lo = x_hi + kPPartBytes;
                 for (int kc = 0; kc < num_kb; kc += kchunk) {
@@ -270,7 +303,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
                         goto mma_done;
                     }
                     tc_fence_after();
-                    const uint32_t d_tmem = tmem_base + acc * kPBN;
+                    const uint32_t d_tmem = tmem_base + acc * kPRowsN;
                     const int kend = kc + kchunk < num_kb ? kc + kchunk : num_kb;
                     for (int kb = kc; kb < kend; ++kb) {
                         if (!mbar_wait(&bars->wfull[r], rph, status, KERR_WAIT_FULL)) {
@@ -278,27 +311,28 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
                             goto mma_done;
                         }
                         tc_fence_after();
-                        const uint32_t a_hi = smem_u32(wring + r * 2 * kPWBytes);
-                        const uint32_t a_lo = a_hi + kPWBytes;
+                        const uint32_t w_hi = smem_u32(wring + r * 2 * kPWBytes);
+                        const uint32_t w_lo = w_hi + kPWBytes;
 #pragma unroll
                         for (int k = 0; k < 4; ++k) {
-                            const uint64_t ad = smem_desc(a_hi + k * 32, 16, 1024, SMEM_SW128);
-                            const uint64_t ad_lo = smem_desc(a_lo + k * 32, 16, 1024, SMEM_SW128);
-                            uint64_t bd, bd_lo;
+                            // weights: K-major, 64 rows of 128 bytes
+                            const uint64_t bd = smem_desc(w_hi + k * 32, 16, 1024, SMEM_SW128);
+                            const uint64_t bd_lo = smem_desc(w_lo + k * 32, 16, 1024, SMEM_SW128);
+                            uint64_t ad, ad_lo;
                             uint32_t idesc;
                             if (st == 0) {  // MN-major, 32-byte atoms (as TMA lands B)
                                 const uint32_t off = kb * kPKbBytes + k * 8 * 128;
-                                bd = smem_desc(x_hi + off, kPBoxBytes, 512, SMEM_SW128_32B);
-                                bd_lo = smem_desc(x_lo + off, kPBoxBytes, 512, SMEM_SW128_32B);
+                                ad = smem_desc(x_hi + off, kPBoxBytes, 512, SMEM_SW128_32B);
+                                ad_lo = smem_desc(x_lo + off, kPBoxBytes, 512, SMEM_SW128_32B);
                                 idesc = kIdescMN;
                             } else {        // K-major (as the epilogue writes it)
                                 const uint32_t off = kb * kPKbBytes + k * 32;
-                                bd = smem_desc(x_hi + off, 16, 1024, SMEM_SW128);
-                                bd_lo = smem_desc(x_lo + off, 16, 1024, SMEM_SW128);
+                                ad = smem_desc(x_hi + off, 16, 1024, SMEM_SW128);
+                                ad_lo = smem_desc(x_lo + off, 16, 1024, SMEM_SW128);
                                 idesc = kIdescK;
                             }
-                            tc_mma<MmaKind::TF32>(c_tmem, ad, bd_lo, idesc, (kb | k) != 0);
-                            tc_mma<MmaKind::TF32>(c_tmem, ad_lo, bd, idesc, 1);
+                            tc_mma<MmaKind::TF32>(c_tmem, ad_lo, bd, idesc, (kb | k) != 0);
+                            tc_mma<MmaKind::TF32>(c_tmem, ad, bd_lo, idesc, 1);
                             tc_mma<MmaKind::TF32>(d_tmem, ad, bd, idesc, (kb != kc || k != 0));
                         }
                         tc_commit(&bars->wempty[r]);
@@ -308,17 +342,18 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
                         }
                     }
                     tc_commit(&bars->acc_full[acc]);
-                    if (++acc == 2) {
+                    if (++acc == kPAcc) {
                         acc = 0;
                         acc_ph ^= 1;
                     }
                 }
                 tc_commit(&bars->corr_full[cb]);
-                if (++cb == 2) {
+                if (++cb == kPCorr) {
                     cb = 0;
                     cb_ph ^= 1;
                 }
                 if (last) tc_commit(&bars->xfree[slot]);  // the buffer may take the next block
+                if (g.trace) ptrace(g, q, st, PT_MMA_END, globaltimer_ns());
                 if (p_aborted(bars)) break;
             }
         mma_done:
@@ -327,27 +362,28 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
         }
     } else {
         // ------------------------------------------------------------ splits and epilogues
-        const int quarter = warp & 3;
-        const int et = threadIdx.x - 64;  // 0..127
-        const int row = quarter * 32 + lane;  // TMEM lane: output row = next stage's k
-        uint8_t *staging = smem + kPStageOff + (warp - 2) * 2 * kStageBufBytes;
-        int sbuf = 0;
+        const int quarter = warp & 3;                // TMEM lanes this warp may read
+        const int col = quarter * 32 + lane;         // this thread's column of the block
+        const int m0 = ((warp - 2) >> 2) * 32;       // its 32 output rows
+        const int et = threadIdx.x - 64;             // 0 .. 32 * kPEpiWarps - 1
+        const uint32_t t_lane = (uint32_t)(quarter * 32) << 16;
         int acc = 0, cb = 0;
         uint32_t acc_ph = 0, cb_ph = 0;
-        int splits[2] = {0, 0};  // stage-0 inputs split per slot: the xin phase to wait for
+        int splits0 = 0, splits1 = 0;  // stage-0 inputs split per slot: the xin phase to wait for
         bool ok = true;
 
         // Split the stage-0 input of the block at position q (in the slot's buffer)
         // into its TF32 (hi, lo) pair in place; then tell the MMA warp.
         auto split = [&](int slot, int q) -> bool {
-            if (!mbar_wait(&bars->xin[slot], (uint32_t)(splits[slot] & 1), status, KERR_WAIT_FULL))
-                return false;
-            ++splits[slot];
+            const bool tr = g.trace && warp == 2 && lane == 0;
+            if (tr) ptrace(g, q, 0, PT_SPLIT_START, globaltimer_ns());
+            const int sp = slot ? splits1++ : splits0++;
+            if (!mbar_wait(&bars->xin[slot], (uint32_t)(sp & 1), status, KERR_WAIT_FULL)) return false;
             const PanelChain &ch = g.chains[g.blocks[q] >> 16];
             const int bytes = ((ch.K[0] + kPBK - 1) / kPBK) * kPKbBytes;
             uint8_t *hi = xbuf + slot * kPSlotBytes;
             uint8_t *lo = hi + kPPartBytes;
-            for (int off = et * 16; off < bytes; off += 128 * 16) {
+            for (int off = et * 16; off < bytes; off += 32 * kPEpiWarps * 16) {
                 const float4 x = *reinterpret_cast<const float4 *>(hi + off);
                 float4 h, l;
                 h.x = f32_to_tf32_rne(x.x); l.x = f32_to_tf32_rne(x.x - h.x);
@@ -360,6 +396,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
             fence_proxy_async_smem();  // generic writes before the MMAs read them
             __syncwarp();
             if (lane == 0) mbar_arrive(&bars->xready[slot]);
+            if (tr) ptrace(g, q, 0, PT_SPLIT_END, globaltimer_ns());
             return true;
         };
 
@@ -374,30 +411,26 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
             const int n0 = (int)(bq & 0xffffu) * kPBN;
             const int num_kb = (ch.K[st] + kPBK - 1) / kPBK;
             const int kchunk = ch.kchunk[st] > 0 ? ch.kchunk[st] : num_kb;
-            float sum[kPBN / 32][32];
+            const bool tr = g.trace && warp == 2 && lane == 0;
+            float sum[32];  // output rows m0 .. m0 + 31 of this thread's column
 #pragma unroll
-            for (int c = 0; c < kPBN / 32; ++c)
-#pragma unroll
-                for (int j = 0; j < 32; ++j) sum[c][j] = 0.f;
+            for (int j = 0; j < 32; ++j) sum[j] = 0.f;
             for (int kc = 0; kc < num_kb; kc += kchunk) {
                 if (!mbar_wait(&bars->acc_full[acc], acc_ph, status, KERR_WAIT_ACC_FULL)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                const uint32_t t_row = tmem_base + acc * kPBN + ((uint32_t)(quarter * 32) << 16);
+                if (tr && kc == 0) ptrace(g, q, st, PT_EPI_START, globaltimer_ns());
+                uint32_t v[32];
+                tmem_ld_32x32b_x32(tmem_base + acc * kPRowsN + m0 + t_lane, v);
+                tmem_ld_wait();
 #pragma unroll
-                for (int c = 0; c < kPBN / 32; ++c) {
-                    uint32_t v[32];
-                    tmem_ld_32x32b_x32(t_row + c * 32, v);
-                    tmem_ld_wait();
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) sum[c][j] = sum[c][j] + __uint_as_float(v[j]);
-                }
+                for (int j = 0; j < 32; ++j) sum[j] = sum[j] + __uint_as_float(v[j]);
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&bars->acc_empty[acc]);
-                if (++acc == 2) {
+                if (++acc == kPAcc) {
                     acc = 0;
                     acc_ph ^= 1;
                 }
@@ -407,70 +440,55 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
             if (!ok) break;
             tc_fence_after();
             {
-                const uint32_t t_row =
-                    tmem_base + 2 * kPBN + cb * kPBN + ((uint32_t)(quarter * 32) << 16);
+                uint32_t w[32];
+                tmem_ld_32x32b_x32(tmem_base + (kPAcc + cb) * kPRowsN + m0 + t_lane, w);
+                tmem_ld_wait();
 #pragma unroll
-                for (int c = 0; c < kPBN / 32; ++c) {
-                    uint32_t w[32];
-                    tmem_ld_32x32b_x32(t_row + c * 32, w);
-                    tmem_ld_wait();
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) sum[c][j] = sum[c][j] + __uint_as_float(w[j]);
-                }
+                for (int j = 0; j < 32; ++j) sum[j] = sum[j] + __uint_as_float(w[j]);
             }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&bars->corr_empty[cb]);
-            if (++cb == 2) {
+            if (++cb == kPCorr) {
                 cb = 0;
                 cb_ph ^= 1;
             }
             const int M = ch.K[st + 1];  // this stage's rows
             if (!last) {
-                // the next stage's (hi, lo) operand, K-major, rows k < round_up(M, 32)
-                // (rows past M hold the zero products of the zero-filled weight rows)
-                if (quarter * 32 < ((M + 31) & ~31)) {
-                    uint8_t *hi = xbuf + slot * kPSlotBytes;
+                // the next stage's (hi, lo) operand: this column's row of the K-major
+                // A operand, k = m0 .. m0 + 31 (one k-block; values past M are the
+                // zero products of the zero-filled weight rows)
+                if (m0 < M) {
+                    uint8_t *hi = xbuf + slot * kPSlotBytes + (m0 / kPBK) * kPKbBytes + col * 128;
                     uint8_t *lo = hi + kPPartBytes;
 #pragma unroll
-                    for (int c = 0; c < kPBN / 32; ++c)
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            const float x = sum[c][j];
-                            const float h = f32_to_tf32_rne(x);
-                            const uint32_t off = kmajor_off(row, c * 32 + j);
-                            *reinterpret_cast<float *>(hi + off) = h;
-                            *reinterpret_cast<float *>(lo + off) = f32_to_tf32_rne(x - h);
-                        }
+                    for (int c = 0; c < 8; ++c) {
+                        float4 h, l;
+                        h.x = f32_to_tf32_rne(sum[4 * c]);     l.x = f32_to_tf32_rne(sum[4 * c] - h.x);
+                        h.y = f32_to_tf32_rne(sum[4 * c + 1]); l.y = f32_to_tf32_rne(sum[4 * c + 1] - h.y);
+                        h.z = f32_to_tf32_rne(sum[4 * c + 2]); l.z = f32_to_tf32_rne(sum[4 * c + 2] - h.z);
+                        h.w = f32_to_tf32_rne(sum[4 * c + 3]); l.w = f32_to_tf32_rne(sum[4 * c + 3] - h.w);
+                        const int sw = (c ^ (col & 7)) << 4;  // 128-byte swizzle of 16-byte chunks
+                        *reinterpret_cast<float4 *>(hi + sw) = h;
+                        *reinterpret_cast<float4 *>(lo + sw) = l;
+                    }
                 }
                 fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&bars->xready[slot]);
+                if (tr) ptrace(g, q, st, PT_EPI_END, globaltimer_ns());
             } else {
-                // the chain's result: staged TMA stores of 32 columns at a time
-                const int warp_row0 = quarter * 32;
-                const bool rows_in = warp_row0 < M;
+                // the chain's result: row m of C gets this column's value; a warp
+                // writes 32 consecutive columns of one row per store
+                const int n = n0 + col;
+                if (n < ch.N) {
+                    float *cp = ch.C + n;
+                    const int mend = M - m0 < 32 ? M - m0 : 32;
 #pragma unroll
-                for (int c = 0; c < kPBN / 32; ++c) {
-                    const int nc = n0 + c * 32;
-                    if (nc >= ch.N) break;  // warp-uniform
-                    uint8_t *b0 = staging + sbuf * kStageBufBytes;
-                    if (lane == 0) bulk_wait_read<1>();  // this buffer's previous store has read it
-                    __syncwarp();
-#pragma unroll
-                    for (int j = 0; j < 8; ++j)
-                        st_sw16(b0, lane, 16 * j,
-                                make_uint4(__float_as_uint(sum[c][4 * j]), __float_as_uint(sum[c][4 * j + 1]),
-                                           __float_as_uint(sum[c][4 * j + 2]),
-                                           __float_as_uint(sum[c][4 * j + 3])));
-                    sbuf ^= 1;
-                    fence_proxy_async_smem();
-                    __syncwarp();
-                    if (lane == 0 && rows_in) {
-                        tma_store_2d(&ch.tm_c, b0, nc, warp_row0);
-                        bulk_commit();
-                    }
+                    for (int j = 0; j < 32; ++j)
+                        if (j < mend) cp[(size_t)(m0 + j) * ch.ldc] = sum[j];
                 }
+                if (tr) ptrace(g, q, st, PT_EPI_END, globaltimer_ns());
                 // this slot's next block, if any: split its stage-0 input
                 const int qn = q + 2;
                 if (qn < walk.q1 && !split(slot, qn)) ok = false;
@@ -480,7 +498,6 @@ __global__ void __launch_bounds__(kThreads, 1) tc_panel_kernel(const __grid_cons
         if (!ok) p_set_abort(bars);
     }
 
-    if (warp >= 2 && lane == 0) bulk_wait<0>();  // staged stores done before shared memory goes
     tc_fence_before();
     __syncthreads();
     if (warp == 1) {
@@ -507,14 +524,13 @@ cudaError_t panel_chain_desc(const PanelChainArgs &a, PanelChain &out)
     if (!make_map(&out.tm_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.B, a.K[0], a.N, a.ldb, kPBoxN,
                   kPBK, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B))
         return cudaErrorInvalidValue;
-    if (!make_map(&out.tm_c, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.C, a.M[a.n - 1], a.N, a.ldc, 32,
-                  32))
-        return cudaErrorInvalidValue;
+    out.C = a.C;
+    out.ldc = a.ldc;
     for (int i = 0; i < a.n; ++i) {
         if (!make_map(&out.tm_w[i][0], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.w_hi[i], a.M[i], a.K[i],
-                      a.ldw[i], kPBK, kBM) ||
+                      a.ldw[i], kPBK, kPRowsN) ||
             !make_map(&out.tm_w[i][1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.w_lo[i], a.M[i], a.K[i],
-                      a.ldw[i], kPBK, kBM))
+                      a.ldw[i], kPBK, kPRowsN))
             return cudaErrorInvalidValue;
         out.K[i] = (int)a.K[i];
         out.kchunk[i] = a.kchunk[i];
@@ -566,7 +582,7 @@ cudaError_t panel_capacity(int num_sms, int &ctas)
                                              kPSmem);
         if (e != cudaSuccess) return e;
         int n = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tc_panel_kernel, kThreads, kPSmem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, tc_panel_kernel, kPThreads, kPSmem);
         if (e != cudaSuccess || n < 1) {
             cudaGetLastError();
             return cudaErrorNotSupported;
@@ -579,14 +595,15 @@ cudaError_t panel_capacity(int num_sms, int &ctas)
 }
 
 cudaError_t launch_panel(const PanelChain *chains_dev, const uint32_t *blocks_dev, const int *off_dev,
-                         int ctas, int *status, cudaStream_t s)
+                         int ctas, int *status, cudaStream_t s, unsigned long long *trace)
 {
     PanelArgs g;
     g.chains = chains_dev;
     g.blocks = blocks_dev;
     g.off = off_dev;
     g.status = status;
-    tc_panel_kernel<<<ctas, kThreads, kPSmem, s>>>(g);
+    g.trace = trace;
+    tc_panel_kernel<<<ctas, kPThreads, kPSmem, s>>>(g);
     return cudaGetLastError();
 }
 
