@@ -380,18 +380,30 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
             const int sp = slot ? splits1++ : splits0++;
             if (!mbar_wait(&bars->xin[slot], (uint32_t)(sp & 1), status, KERR_WAIT_FULL)) return false;
             const PanelChain &ch = g.chains[g.blocks[q] >> 16];
-            const int bytes = ((ch.K[0] + kPBK - 1) / kPBK) * kPKbBytes;
+            const int kbs = (ch.K[0] + kPBK - 1) / kPBK;
             uint8_t *hi = xbuf + slot * kPSlotBytes;
             uint8_t *lo = hi + kPPartBytes;
-            for (int off = et * 16; off < bytes; off += 32 * kPEpiWarps * 16) {
-                const float4 x = *reinterpret_cast<const float4 *>(hi + off);
-                float4 h, l;
-                h.x = f32_to_tf32_rne(x.x); l.x = f32_to_tf32_rne(x.x - h.x);
-                h.y = f32_to_tf32_rne(x.y); l.y = f32_to_tf32_rne(x.y - h.y);
-                h.z = f32_to_tf32_rne(x.z); l.z = f32_to_tf32_rne(x.z - h.z);
-                h.w = f32_to_tf32_rne(x.w); l.w = f32_to_tf32_rne(x.w - h.w);
-                *reinterpret_cast<float4 *>(hi + off) = h;
-                *reinterpret_cast<float4 *>(lo + off) = l;
+            constexpr int kStep = 32 * kPEpiWarps * 16;       // bytes per pass of all threads
+            constexpr int kPer = kPKbBytes / kStep;            // passes per k-block
+#pragma unroll
+            for (int kb = 0; kb < kPKb; ++kb) {
+                if (kb < kbs) {
+                    float4 x[kPer];
+#pragma unroll
+                    for (int i = 0; i < kPer; ++i)
+                        x[i] = *reinterpret_cast<const float4 *>(hi + kb * kPKbBytes + i * kStep + et * 16);
+#pragma unroll
+                    for (int i = 0; i < kPer; ++i) {
+                        float4 h, l;
+                        h.x = f32_to_tf32_rne(x[i].x); l.x = f32_to_tf32_rne(x[i].x - h.x);
+                        h.y = f32_to_tf32_rne(x[i].y); l.y = f32_to_tf32_rne(x[i].y - h.y);
+                        h.z = f32_to_tf32_rne(x[i].z); l.z = f32_to_tf32_rne(x[i].z - h.z);
+                        h.w = f32_to_tf32_rne(x[i].w); l.w = f32_to_tf32_rne(x[i].w - h.w);
+                        const int off = kb * kPKbBytes + i * kStep + et * 16;
+                        *reinterpret_cast<float4 *>(hi + off) = h;
+                        *reinterpret_cast<float4 *>(lo + off) = l;
+                    }
+                }
             }
             fence_proxy_async_smem();  // generic writes before the MMAs read them
             __syncwarp();

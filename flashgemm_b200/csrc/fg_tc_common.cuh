@@ -113,13 +113,16 @@ __device__ __forceinline__ uint16_t f32_to_bf16_rne(float f)
     return (uint16_t)(u >> 16);
 }
 
-// Round FP32 to the nearest TF32 value (10 explicit mantissa bits), ties to even.
+// Round FP32 to the nearest TF32 value (10 explicit mantissa bits), ties to
+// even, as an FP32 bit pattern with the low 13 bits clear: one cvt.rn.tf32.f32.
+// For every finite input this equals rounding the low 13 bits of the pattern
+// as an integer (add 0xfff plus bit 13, clear the low bits); that was checked
+// on B200 over all 2^32 patterns.
 __device__ __forceinline__ float f32_to_tf32_rne(float f)
 {
-    uint32_t u = __float_as_uint(f);
-    if ((u & 0x7f800000u) == 0x7f800000u) return f;
-    u += 0xfffu + ((u >> 13) & 1u);
-    return __uint_as_float(u & 0xffffe000u);
+    uint32_t r;
+    asm("cvt.rn.tf32.f32 %0, %1;" : "=r"(r) : "f"(f));
+    return __uint_as_float(r);
 }
 
 __device__ __forceinline__ int8_t sat_s8(int32_t v)
