@@ -690,34 +690,19 @@ int run_chain(DevCtx *c, int dtype, int sem, int algo, void *C, long ldc, Mat b,
                 pa.K[i] = K[i];
                 pa.kchunk[i] = tf32_chunk_blocks(K[i]);
             }
-            GroupExec gx;
-            gx.panel.resize(1);
-            cudaError_t e = panel_chain_desc(pa, gx.panel[0]);
-            if (e != cudaSuccess) return fail(FG_ERR_INVALID, "panel tables: %s", cudaGetErrorString(e));
             double fl = 0.0;
             for (int i = 0; i < n; ++i) fl += gemm_flops(M[i], N, K[i]);
-            int st = panel_finish(c, gx);
-            if (st) return st;
-            PanelChain *pd = (PanelChain *)arena_take(c, sizeof(PanelChain));
-            uint32_t *bd = (uint32_t *)arena_take(c, gx.panel_blocks.size() * sizeof(uint32_t));
-            int *od = (int *)arena_take(c, gx.panel_off.size() * sizeof(int));
-            CUDA_TRY(cudaMemcpyAsync(pd, gx.panel.data(), sizeof(PanelChain), cudaMemcpyHostToDevice,
-                                     c->work));
-            CUDA_TRY(cudaMemcpyAsync(bd, gx.panel_blocks.data(),
-                                     gx.panel_blocks.size() * sizeof(uint32_t),
-                                     cudaMemcpyHostToDevice, c->work));
-            CUDA_TRY(cudaMemcpyAsync(od, gx.panel_off.data(), gx.panel_off.size() * sizeof(int),
-                                     cudaMemcpyHostToDevice, c->work));
+            const long nblocks = (N + 127) / 128;
             // FG_TRACE_DIR=<dir>: a per-tile timeline of every panel launch
             static const char *trace_dir = getenv("FG_TRACE_DIR");
-            const size_t trace_words = gx.panel_blocks.size() * kPanelMaxStages * kPanelTraceFields;
+            const size_t trace_words = (size_t)nblocks * kPanelMaxStages * kPanelTraceFields;
             unsigned long long *trace = nullptr;
             if (trace_dir) {
                 trace = (unsigned long long *)arena_take(c, trace_words * 8);
                 CUDA_TRY(cudaMemsetAsync(trace, 0, trace_words * 8, c->work));
             }
-            st = run_kernel(c, FG_PK_TC_TF32X3, fl, "panel-resident chain", [&] {
-                return launch_panel(pd, bd, od, gx.panel_ctas, c->status, c->work, trace);
+            int st = run_kernel(c, FG_PK_TC_TF32X3, fl, "panel-resident chain", [&] {
+                return launch_panel_one(pa, c->sms, c->status, c->work, trace);
             });
             if (st == FG_OK && trace) {
                 std::vector<unsigned long long> h(trace_words);

@@ -237,7 +237,9 @@ struct alignas(64) PanelChain {
     int kchunk[kPanelMaxStages];             // k-blocks per FP32 promotion of the partial sum
 };
 
-// One launch: every CTA runs blocks[off[cta] .. off[cta + 1]) (chain << 16 | block).
+// One launch: every CTA runs blocks[off[cta] .. off[cta + 1]) (chain << 16 | block);
+// or, with blocks null, the single chain `one` (carried in the parameters), CTA
+// u running its blocks u, u + grid, u + 2 grid, ...
 struct PanelArgs {
     const PanelChain *chains;
     const uint32_t *blocks;
@@ -246,6 +248,8 @@ struct PanelArgs {
     // optional (else null): kPanelTraceFields %globaltimer stamps per
     // (block position, stage), rows at (position * kPanelMaxStages + stage)
     unsigned long long *trace;
+    int one_blocks;      // blocks of `one`
+    PanelChain one;
 };
 constexpr int kPanelTraceFields = 10;
 
@@ -273,6 +277,11 @@ cudaError_t panel_capacity(int num_sms, int &ctas);
 cudaError_t launch_panel(const PanelChain *chains_dev, const uint32_t *blocks_dev, const int *off_dev,
                          int ctas, int *status, cudaStream_t s,
                          unsigned long long *trace = nullptr);
+// One chain, its description in the launch parameters (no tables): the
+// description of the last few operand sets is kept, so repeat calls encode no
+// tensor maps.
+cudaError_t launch_panel_one(const PanelChainArgs &a, int num_sms, int *status, cudaStream_t s,
+                             unsigned long long *trace = nullptr);
 
 // Plain FP32 SGEMM on CUDA cores: C = A * B, one FMA per k in increasing k;
 // with kblock > 0 each block of kblock k is summed from zero and added to C.
