@@ -17,7 +17,8 @@
 // the next stage's A operand (16-byte stores into shared memory); for the last
 // stage it stores them to global memory, each warp writing 32 consecutive
 // columns of an output row at a time. Weights (a few KB per stage) stream from
-// L2 through a TMA ring as the B operand.
+// L2 through a TMA ring as the B operand, and the next block's input loads into
+// a prefetch buffer while the blocks in flight compute.
 //
 // The arithmetic is the grouped 3xTF32 kernel's (fg_group.cu) with the operand
 // roles exchanged: per 32-deep k-block four K = 8 MMAs, each the correction
@@ -58,13 +59,14 @@ constexpr int kPPartBytes = kPKb * kPKbBytes;  // hi or lo of one block: 32 KB
 constexpr int kPSlotBytes = 2 * kPPartBytes;   // (hi, lo) of one block in flight
 constexpr int kPRowsN = kPanelKMax;            // MMA N: output rows of a stage (padded)
 constexpr int kPWBytes = kPRowsN * 128;        // one k-block of weights: 64 rows x 128 B
-constexpr int kPRing = 6;                      // weight ring slots, each (hi, lo)
+constexpr int kPRing = 4;                      // weight ring slots, each (hi, lo)
 constexpr int kPEpiWarps = 16;                 // four per TMEM lane quarter
 constexpr int kPSlice = kPRowsN * 4 / kPEpiWarps;  // output rows per epilogue warp: 16
 constexpr int kPThreads = 64 + 32 * kPEpiWarps;
 constexpr int kPXOff = 0;
 constexpr int kPWOff = kPXOff + 2 * kPSlotBytes;
-constexpr int kPBarOff = kPWOff + kPRing * 2 * kPWBytes;
+constexpr int kPPfOff = kPWOff + kPRing * 2 * kPWBytes;  // next block's stage-0 input, as loaded
+constexpr int kPBarOff = kPPfOff + kPPartBytes;
 constexpr int kPSmem = kPBarOff + 512 + 1024;  // + barriers + alignment slack
 constexpr int kPAcc = 4;                       // partial-sum accumulators (one per FP32 chunk)
 constexpr int kPCorr = 4;                      // correction accumulators (one per tile)
@@ -81,9 +83,9 @@ constexpr uint32_t kIdescK = make_idesc(1, 2, 2, 0, 0, kPBN, kPRowsN);
 
 struct __align__(8) PanelBars {
     uint64_t wfull[kPRing], wempty[kPRing];   // weight ring
-    uint64_t xin[2];      // stage-0 input of a block landed in its operand buffer (TMA bytes)
+    uint64_t pf_full;     // a block's stage-0 input landed in the prefetch buffer (TMA bytes)
+    uint64_t pf_empty;    // the epilogue warps have split it out (kPEpiWarps arrivals)
     uint64_t xready[2];   // the operand buffer holds the next tile's A (kPEpiWarps arrivals)
-    uint64_t xfree[2];    // the MMAs of a block's last stage are done: the buffer may refill
     uint64_t acc_full[kPAcc], acc_empty[kPAcc];      // partial-sum accumulators
     uint64_t corr_full[kPCorr], corr_empty[kPCorr];  // correction accumulators
     uint64_t mma_done;
@@ -194,9 +196,7 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
             mbar_init(&bars->wempty[r], 1);
         }
         for (int s = 0; s < 2; ++s) {
-            mbar_init(&bars->xin[s], 1);
             mbar_init(&bars->xready[s], kPEpiWarps);
-            mbar_init(&bars->xfree[s], 1);
         }
         for (int a = 0; a < kPAcc; ++a) {
             mbar_init(&bars->acc_full[a], 1);
@@ -206,6 +206,8 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
             mbar_init(&bars->corr_full[a], 1);
             mbar_init(&bars->corr_empty[a], kPEpiWarps);
         }
+        mbar_init(&bars->pf_full, 1);
+        mbar_init(&bars->pf_empty, kPEpiWarps);
         mbar_init(&bars->mma_done, 1);
         bars->abort = 0;
         fence_mbar_init();
@@ -225,9 +227,8 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
             int r = 0;
             uint32_t rph = 0;
             uint32_t pending = 0, pending_ph = 0;  // ring slots with loads in flight
-            uint32_t xin_pending = 0;              // operand buffers with a load in flight
-            uint32_t xin_ph0 = 0, xin_ph1 = 0;
-            int loaded0 = 0, loaded1 = 0;          // blocks loaded into each buffer so far
+            int pf_loads = 0;                      // blocks loaded into the prefetch buffer
+            uint32_t pf_ph = 0;                    // the last load's pf_full phase
             int slot, q, st;
             bool last;
             while (walk.next(slot, q, st, last)) {
@@ -241,31 +242,25 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
                     ptrace(g, q, st, PT_PROD_START, globaltimer_ns());
                 }
                 if (st == 0) {
-                    // this block's B into the slot's buffer once the slot's previous
-                    // block's last MMAs are done
-                    const int loaded = slot ? loaded1 : loaded0;
-                    if (!mbar_wait(&bars->xfree[slot], (uint32_t)(loaded & 1) ^ 1u, status,
+                    // this block's B into the prefetch buffer once the epilogue warps
+                    // have split the previous block's out of it (so the load runs while
+                    // the blocks in flight still compute)
+                    if (!mbar_wait(&bars->pf_empty, (uint32_t)(pf_loads & 1) ^ 1u, status,
                                    KERR_WAIT_EMPTY)) {
                         p_set_abort(bars);
                         goto producer_done;
                     }
-                    if (slot) {
-                        ++loaded1;
-                        xin_ph1 = (uint32_t)(loaded & 1);
-                    } else {
-                        ++loaded0;
-                        xin_ph0 = (uint32_t)(loaded & 1);
-                    }
+                    pf_ph = (uint32_t)(pf_loads & 1);
+                    ++pf_loads;
                     const int nkb = (ch.K[0] + kPBK - 1) / kPBK;
                     int nvb = (ch.N - n0 + kPBoxN - 1) / kPBoxN;  // boxes that start inside N
                     nvb = nvb < kPBN / kPBoxN ? nvb : kPBN / kPBoxN;
-                    mbar_arrive_expect_tx(&bars->xin[slot], (uint32_t)(nkb * nvb * kPBoxBytes));
-                    uint8_t *x = xbuf + slot * kPSlotBytes;
+                    mbar_arrive_expect_tx(&bars->pf_full, (uint32_t)(nkb * nvb * kPBoxBytes));
+                    uint8_t *x = smem + kPPfOff;
                     for (int kb = 0; kb < nkb; ++kb)
                         for (int j = 0; j < nvb; ++j)
-                            tma_load_2d(x + kb * kPKbBytes + j * kPBoxBytes, &ch.tm_b, &bars->xin[slot],
+                            tma_load_2d(x + kb * kPKbBytes + j * kPBoxBytes, &ch.tm_b, &bars->pf_full,
                                         n0 + j * kPBoxN, kb * kPBK);
-                    xin_pending |= 1u << slot;
                 }
                 const int nkb = (ch.K[st] + kPBK - 1) / kPBK;
                 for (int kb = 0; kb < nkb; ++kb) {
@@ -292,8 +287,7 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
             for (int i = 0; i < kPRing; ++i)
                 if (pending & (1u << i))
                     mbar_wait(&bars->wfull[i], (pending_ph >> i) & 1u, status, KERR_WAIT_FULL);
-            if (xin_pending & 1u) mbar_wait(&bars->xin[0], xin_ph0, status, KERR_WAIT_FULL);
-            if (xin_pending & 2u) mbar_wait(&bars->xin[1], xin_ph1, status, KERR_WAIT_FULL);
+            if (pf_loads) mbar_wait(&bars->pf_full, pf_ph, status, KERR_WAIT_FULL);
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
@@ -378,7 +372,6 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
                     cb = 0;
                     cb_ph ^= 1;
                 }
-                if (last) tc_commit(&bars->xfree[slot]);  // the buffer may take the next block
                 if (g.trace) ptrace(g, q, st, PT_MMA_END, globaltimer_ns());
                 if (p_aborted(bars)) break;
             }
@@ -395,18 +388,21 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
         const uint32_t t_lane = (uint32_t)(quarter * 32) << 16;
         int acc = 0, cb = 0;
         uint32_t acc_ph = 0, cb_ph = 0;
-        int splits0 = 0, splits1 = 0;  // stage-0 inputs split per slot: the xin phase to wait for
+        int splits = 0;  // stage-0 inputs split so far: the pf_full phase to wait for
         bool ok = true;
 
-        // Split the stage-0 input of the block at position q (in the slot's buffer)
-        // into its TF32 (hi, lo) pair in place; then tell the MMA warp.
+        // Split the stage-0 input of the block at position q (in the prefetch
+        // buffer) into its TF32 (hi, lo) pair in the slot's operand buffer (free:
+        // the slot's previous block is done); then free the prefetch buffer and
+        // tell the MMA warp.
         auto split = [&](int slot, int q) -> bool {
             const bool tr = g.trace && warp == 2 && lane == 0;
             if (tr) ptrace(g, q, 0, PT_SPLIT_START, globaltimer_ns());
-            const int sp = slot ? splits1++ : splits0++;
-            if (!mbar_wait(&bars->xin[slot], (uint32_t)(sp & 1), status, KERR_WAIT_FULL)) return false;
+            const int sp = splits++;
+            if (!mbar_wait(&bars->pf_full, (uint32_t)(sp & 1), status, KERR_WAIT_FULL)) return false;
             const PanelChain &ch = chain_of(g, blk(g, q));
             const int kbs = (ch.K[0] + kPBK - 1) / kPBK;
+            const uint8_t *pf = smem + kPPfOff;
             uint8_t *hi = xbuf + slot * kPSlotBytes;
             uint8_t *lo = hi + kPPartBytes;
             constexpr int kStep = 32 * kPEpiWarps * 16;       // bytes per pass of all threads
@@ -417,7 +413,7 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
                     float4 x[kPer];
 #pragma unroll
                     for (int i = 0; i < kPer; ++i)
-                        x[i] = *reinterpret_cast<const float4 *>(hi + kb * kPKbBytes + i * kStep + et * 16);
+                        x[i] = *reinterpret_cast<const float4 *>(pf + kb * kPKbBytes + i * kStep + et * 16);
 #pragma unroll
                     for (int i = 0; i < kPer; ++i) {
                         float4 h, l;
@@ -433,7 +429,10 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
             }
             fence_proxy_async_smem();  // generic writes before the MMAs read them
             __syncwarp();
-            if (lane == 0) mbar_arrive(&bars->xready[slot]);
+            if (lane == 0) {
+                mbar_arrive(&bars->pf_empty);
+                mbar_arrive(&bars->xready[slot]);
+            }
             if (tr) ptrace(g, q, 0, PT_SPLIT_END, globaltimer_ns());
             return true;
         };
