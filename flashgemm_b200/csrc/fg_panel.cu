@@ -68,9 +68,15 @@ constexpr int kPWOff = kPXOff + 2 * kPSlotBytes;
 constexpr int kPPfOff = kPWOff + kPRing * 2 * kPWBytes;  // next block's stage-0 input, as loaded
 constexpr int kPBarOff = kPPfOff + kPPartBytes;
 constexpr int kPSmem = kPBarOff + 512 + 1024;  // + barriers + alignment slack
-constexpr int kPAcc = 4;                       // partial-sum accumulators (one per FP32 chunk)
-constexpr int kPCorr = 4;                      // correction accumulators (one per tile)
-constexpr int kPTmemCols = (kPAcc + kPCorr) * kPRowsN;
+// A tile's accumulators, one set of [d0 | c | d1] (kPRowsN columns each): the
+// partial sums of its FP32 chunks (at most two: K <= 64) around the correction
+// term, so that an N = 2 * kPRowsN MMA over stacked (hi, lo) weights writes the
+// correction and a partial sum at once. Two sets: two tiles in flight.
+constexpr int kPSets = 2;
+constexpr int kPSetCols = 3 * kPRowsN;
+constexpr int kPTmemCols = 512;
+static_assert(kPSets * kPSetCols <= kPTmemCols, "TMEM columns");
+static_assert(kPKb == 2, "at most two k-blocks, so at most two FP32 chunks");
 static_assert(kPSmem <= 232448, "shared memory per CTA");
 static_assert(kPTmemCols == 512, "TMEM allocation: a power of two");
 static_assert(kPSlice == 16 && kPBK % kPSlice == 0, "a warp's rows lie in one k-block");
@@ -80,14 +86,17 @@ static_assert(kPSlice == 16 && kPBK % kPSlice == 0, "a warp's rows lie in one k-
 // K-major); M = 128 columns, N = 64 output rows
 constexpr uint32_t kIdescMN = make_idesc(1, 2, 2, 1, 0, kPBN, kPRowsN);
 constexpr uint32_t kIdescK = make_idesc(1, 2, 2, 0, 0, kPBN, kPRowsN);
+constexpr uint32_t kIdescMN2 = make_idesc(1, 2, 2, 1, 0, kPBN, 2 * kPRowsN);  // stacked weights
+constexpr uint32_t kIdescK2 = make_idesc(1, 2, 2, 0, 0, kPBN, 2 * kPRowsN);
 
 struct __align__(8) PanelBars {
     uint64_t wfull[kPRing], wempty[kPRing];   // weight ring
     uint64_t pf_full;     // a block's stage-0 input landed in the prefetch buffer (TMA bytes)
     uint64_t pf_empty;    // the epilogue warps have split it out (kPEpiWarps arrivals)
     uint64_t xready[2];   // the operand buffer holds the next tile's A (kPEpiWarps arrivals)
-    uint64_t acc_full[kPAcc], acc_empty[kPAcc];      // partial-sum accumulators
-    uint64_t corr_full[kPCorr], corr_empty[kPCorr];  // correction accumulators
+    uint64_t first_full[kPSets];  // a set's first chunk (d0) is final
+    uint64_t set_full[kPSets];    // all of a set (d1, c) is final
+    uint64_t set_empty[kPSets];   // the epilogue warps have read the set
     uint64_t mma_done;
     uint32_t tmem_base;
     int abort;
@@ -198,13 +207,10 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
         for (int s = 0; s < 2; ++s) {
             mbar_init(&bars->xready[s], kPEpiWarps);
         }
-        for (int a = 0; a < kPAcc; ++a) {
-            mbar_init(&bars->acc_full[a], 1);
-            mbar_init(&bars->acc_empty[a], kPEpiWarps);
-        }
-        for (int a = 0; a < kPCorr; ++a) {
-            mbar_init(&bars->corr_full[a], 1);
-            mbar_init(&bars->corr_empty[a], kPEpiWarps);
+        for (int a = 0; a < kPSets; ++a) {
+            mbar_init(&bars->first_full[a], 1);
+            mbar_init(&bars->set_full[a], 1);
+            mbar_init(&bars->set_empty[a], kPEpiWarps);
         }
         mbar_init(&bars->pf_full, 1);
         mbar_init(&bars->pf_empty, kPEpiWarps);
@@ -263,15 +269,21 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
                                         n0 + j * kPBoxN, kb * kPBK);
                 }
                 const int nkb = (ch.K[st] + kPBK - 1) / kPBK;
+                const int kchunk = ch.kchunk[st] > 0 ? ch.kchunk[st] : nkb;
                 for (int kb = 0; kb < nkb; ++kb) {
                     if (!mbar_wait(&bars->wempty[r], rph ^ 1, status, KERR_WAIT_EMPTY)) {
                         p_set_abort(bars);
                         goto producer_done;
                     }
+                    // stacked (hi, lo) for the first chunk's k-blocks, (lo, hi) for the
+                    // second's: the stacked MMA writes [d0 | c] or [c | d1]
+                    const bool lo_first = ((kb / kchunk) & 1) != 0;
                     uint8_t *w = wring + r * 2 * kPWBytes;
                     mbar_arrive_expect_tx(&bars->wfull[r], 2u * kPWBytes);
-                    tma_load_2d(w, &ch.tm_w[st][0], &bars->wfull[r], kb * kPBK, 0);
-                    tma_load_2d(w + kPWBytes, &ch.tm_w[st][1], &bars->wfull[r], kb * kPBK, 0);
+                    tma_load_2d(w + (lo_first ? kPWBytes : 0), &ch.tm_w[st][0], &bars->wfull[r],
+                                kb * kPBK, 0);
+                    tma_load_2d(w + (lo_first ? 0 : kPWBytes), &ch.tm_w[st][1], &bars->wfull[r],
+                                kb * kPBK, 0);
                     pending |= 1u << r;
                     pending_ph = (pending_ph & ~(1u << r)) | (rph << r);
                     if (++r == kPRing) {
@@ -294,8 +306,7 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
         if (lane == 0) {
             int r = 0;
             uint32_t rph = 0;
-            int acc = 0, cb = 0;
-            uint32_t acc_ph = 0, cb_ph = 0;
+            int sets = 0;                // tiles issued: set sets % kPSets, phase (sets / kPSets) & 1
             int tiles0 = 0, tiles1 = 0;  // tiles issued per slot: the xready phase to wait for
             int slot, q, st;
             bool last;
@@ -307,16 +318,19 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
                     p_set_abort(bars);
                     goto mma_done;
                 }
-                tc_fence_after();
-                const int num_kb = (ch.K[st] + kPBK - 1) / kPBK;
-                const int kchunk = ch.kchunk[st] > 0 ? ch.kchunk[st] : num_kb;
-                if (!mbar_wait(&bars->corr_empty[cb], cb_ph ^ 1, status, KERR_WAIT_ACC_EMPTY)) {
+                const int set = sets % kPSets;
+                const uint32_t set_ph = (uint32_t)((sets / kPSets) & 1);
+                ++sets;
+                if (!mbar_wait(&bars->set_empty[set], set_ph ^ 1u, status, KERR_WAIT_ACC_EMPTY)) {
                     p_set_abort(bars);
                     goto mma_done;
                 }
                 tc_fence_after();
                 if (g.trace) ptrace(g, q, st, PT_MMA_START, globaltimer_ns());
-                const uint32_t c_tmem = tmem_base + (kPAcc + cb) * kPRowsN;
+                const int num_kb = (ch.K[st] + kPBK - 1) / kPBK;
+                const int kchunk = ch.kchunk[st] > 0 ? ch.kchunk[st] : num_kb;
+                const uint32_t s_tmem = tmem_base + set * kPSetCols;  // [d0 | c | d1]
+                const uint32_t c_tmem = s_tmem + kPRowsN;
                 // descriptors of k-step 0, built once per tile: a k-step, a k-block
                 // and the lo part only move the start address (field: bytes >> 4)
                 const uint32_t x_hi = smem_u32(xbuf + slot * kPSlotBytes);
@@ -325,14 +339,12 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
                                        : smem_desc(x_hi, 16, 1024, SMEM_SW128);
                 const uint64_t a_step = mn ? (8 * 128) >> 4 : 32 >> 4;
                 const uint32_t idesc = mn ? kIdescMN : kIdescK;
+                const uint32_t idesc2 = mn ? kIdescMN2 : kIdescK2;
                 const uint64_t w0 = smem_desc(smem_u32(wring), 16, 1024, SMEM_SW128);
                 for (int kc = 0; kc < num_kb; kc += kchunk) {
-                    if (!mbar_wait(&bars->acc_empty[acc], acc_ph ^ 1, status, KERR_WAIT_ACC_EMPTY)) {
-                        p_set_abort(bars);
-                        goto mma_done;
-                    }
-                    tc_fence_after();
-                    const uint32_t d_tmem = tmem_base + acc * kPRowsN;
+                    const bool second = kc > 0;  // the tile's second FP32 chunk
+                    const uint32_t d_tmem = second ? s_tmem + 2 * kPRowsN : s_tmem;
+                    const uint32_t stack_tmem = second ? c_tmem : s_tmem;  // [c | d1] or [d0 | c]
                     const int kend = kc + kchunk < num_kb ? kc + kchunk : num_kb;
                     for (int kb = kc; kb < kend; ++kb) {
                         if (!mbar_wait(&bars->wfull[r], rph, status, KERR_WAIT_FULL)) {
@@ -342,18 +354,25 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
                         tc_fence_after();
                         const uint64_t ak = a0 + (uint64_t)(kb * (kPKbBytes >> 4));
                         const uint64_t ak_lo = ak + (kPPartBytes >> 4);
-                        const uint64_t bk = w0 + (uint64_t)(r * ((2 * kPWBytes) >> 4));  // weights hi
-                        const uint64_t bk_lo = bk + (kPWBytes >> 4);
+                        const uint64_t bst = w0 + (uint64_t)(r * ((2 * kPWBytes) >> 4));  // stacked
+                        const uint64_t bk = second ? bst + (kPWBytes >> 4) : bst;           // hi
+                        const uint64_t bk_lo = second ? bst : bst + (kPWBytes >> 4);        // lo
 #pragma unroll
                         for (int k = 0; k < 4; ++k) {
-                            // the partial-sum MMA between the two correction MMAs: the
-                            // accumulators' summation orders are unchanged, and no two
-                            // MMAs in a row accumulate into the same columns
-                            tc_mma<MmaKind::TF32>(c_tmem, ak_lo + k * a_step, bk + k * 2, idesc,
-                                                  (kb | k) != 0);
-                            tc_mma<MmaKind::TF32>(d_tmem, ak + k * a_step, bk + k * 2, idesc,
-                                                  (kb != kc || k != 0));
-                            tc_mma<MmaKind::TF32>(c_tmem, ak + k * a_step, bk_lo + k * 2, idesc, 1);
+                            if (kb == kc && k == 0) {
+                                // a chunk's first k-step: its partial sum starts here, the
+                                // correction accumulates on (three MMAs, the partial-sum
+                                // one between the correction ones)
+                                tc_mma<MmaKind::TF32>(c_tmem, ak_lo, bk, idesc, kb != 0);
+                                tc_mma<MmaKind::TF32>(d_tmem, ak, bk, idesc, 0);
+                                tc_mma<MmaKind::TF32>(c_tmem, ak, bk_lo, idesc, 1);
+                            } else {
+                                // lo*hi into the correction, then one MMA over the stacked
+                                // weights: hi*lo into the correction and hi*hi into the
+                                // partial sum (each accumulator's order as above)
+                                tc_mma<MmaKind::TF32>(c_tmem, ak_lo + k * a_step, bk + k * 2, idesc, 1);
+                                tc_mma<MmaKind::TF32>(stack_tmem, ak + k * a_step, bst + k * 2, idesc2, 1);
+                            }
                         }
                         tc_commit(&bars->wempty[r]);
                         if (++r == kPRing) {
@@ -361,17 +380,9 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
                             rph ^= 1;
                         }
                     }
-                    tc_commit(&bars->acc_full[acc]);
-                    if (++acc == kPAcc) {
-                        acc = 0;
-                        acc_ph ^= 1;
-                    }
+                    if (!second) tc_commit(&bars->first_full[set]);
                 }
-                tc_commit(&bars->corr_full[cb]);
-                if (++cb == kPCorr) {
-                    cb = 0;
-                    cb_ph ^= 1;
-                }
+                tc_commit(&bars->set_full[set]);
                 if (g.trace) ptrace(g, q, st, PT_MMA_END, globaltimer_ns());
                 if (p_aborted(bars)) break;
             }
@@ -386,8 +397,7 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
         const int m0 = ((warp - 2) >> 2) * kPSlice;  // its output rows m0 .. m0 + kPSlice - 1
         const int et = threadIdx.x - 64;             // 0 .. 32 * kPEpiWarps - 1
         const uint32_t t_lane = (uint32_t)(quarter * 32) << 16;
-        int acc = 0, cb = 0;
-        uint32_t acc_ph = 0, cb_ph = 0;
+        int sets = 0;    // tiles read: set sets % kPSets, phase (sets / kPSets) & 1
         int splits = 0;  // stage-0 inputs split so far: the pf_full phase to wait for
         bool ok = true;
 
@@ -452,44 +462,46 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
             float sum[kPSlice];  // output rows m0 .. of this thread's column
 #pragma unroll
             for (int j = 0; j < kPSlice; ++j) sum[j] = 0.f;
-            for (int kc = 0; kc < num_kb; kc += kchunk) {
-                if (!mbar_wait(&bars->acc_full[acc], acc_ph, status, KERR_WAIT_ACC_FULL)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                if (tr && kc == 0) ptrace(g, q, st, PT_EPI_START, globaltimer_ns());
+            const int set = sets % kPSets;
+            const uint32_t set_ph = (uint32_t)((sets / kPSets) & 1);
+            ++sets;
+            const uint32_t s_tmem = tmem_base + set * kPSetCols + m0 + t_lane;  // [d0 | c | d1]
+            // the first chunk's partial sum, then the second's, then the correction
+            if (!mbar_wait(&bars->first_full[set], set_ph, status, KERR_WAIT_ACC_FULL)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            if (tr) ptrace(g, q, st, PT_EPI_START, globaltimer_ns());
+            {
                 uint32_t v[kPSlice];
-                tmem_ld_32x32b_x16(tmem_base + acc * kPRowsN + m0 + t_lane, v);
+                tmem_ld_32x32b_x16(s_tmem, v);
                 tmem_ld_wait();
 #pragma unroll
                 for (int j = 0; j < kPSlice; ++j) sum[j] = sum[j] + __uint_as_float(v[j]);
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&bars->acc_empty[acc]);
-                if (++acc == kPAcc) {
-                    acc = 0;
-                    acc_ph ^= 1;
-                }
             }
-            // the tile's correction terms, added once
-            if (ok && !mbar_wait(&bars->corr_full[cb], cb_ph, status, KERR_WAIT_ACC_FULL)) ok = false;
-            if (!ok) break;
+            if (!mbar_wait(&bars->set_full[set], set_ph, status, KERR_WAIT_ACC_FULL)) {
+                ok = false;
+                break;
+            }
             tc_fence_after();
+            if (kchunk < num_kb) {
+                uint32_t v[kPSlice];
+                tmem_ld_32x32b_x16(s_tmem + 2 * kPRowsN, v);
+                tmem_ld_wait();
+#pragma unroll
+                for (int j = 0; j < kPSlice; ++j) sum[j] = sum[j] + __uint_as_float(v[j]);
+            }
             {
                 uint32_t w[kPSlice];
-                tmem_ld_32x32b_x16(tmem_base + (kPAcc + cb) * kPRowsN + m0 + t_lane, w);
+                tmem_ld_32x32b_x16(s_tmem + kPRowsN, w);
                 tmem_ld_wait();
 #pragma unroll
                 for (int j = 0; j < kPSlice; ++j) sum[j] = sum[j] + __uint_as_float(w[j]);
             }
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&bars->corr_empty[cb]);
-            if (++cb == kPCorr) {
-                cb = 0;
-                cb_ph ^= 1;
-            }
+            if (lane == 0) mbar_arrive(&bars->set_empty[set]);
             const int M = ch.K[st + 1];  // this stage's rows
             if (!last) {
                 // the next stage's (hi, lo) operand: this column's row of the K-major
