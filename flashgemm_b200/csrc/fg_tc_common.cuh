@@ -449,7 +449,12 @@ __device__ __forceinline__ void drain_staged(const StageArgs &p, const CUtensorM
         fence_proxy_async_smem();
         __syncwarp();
         if (lane == 0 && rows_in) {
-            tma_store_2d(tm_out, sb, col0, warp_row0);
+            // a chain's result is not read again in the launch: first out of L2, so
+            // that the intermediates the next stages read stay in it
+            if constexpr (EPI == EPI_BF16 || EPI == EPI_S8)
+                tma_store_2d(tm_out, sb, col0, warp_row0);
+            else
+                tma_store_2d_hint(tm_out, sb, col0, warp_row0, l2_policy_evict_first());
             bulk_commit();
         }
         sbuf ^= 1;
