@@ -975,6 +975,88 @@ class GpuCtx:
             self.dist.destroy_process_group()
 
 
+# The reference's own three-stage chain table (multigemm/test/test_bf16_3.c:14-48; the
+# FP32 and INT8 tests use the same shapes): N, K_1, (M_1, M_2, M_3)
+REF_CHAINS = [
+    (65536, 288, (32, 24, 144)), (16384, 1296, (144, 32, 192)), (16384, 1728, (192, 32, 192)),
+    (4096, 4800, (192, 56, 336)), (4096, 8400, (336, 56, 336)), (50176, 288, (32, 16, 96)),
+    (12544, 864, (96, 24, 144)), (12544, 1296, (144, 24, 144)), (3136, 1296, (144, 32, 192)),
+    (3136, 1728, (192, 32, 192)),
+]
+
+
+def run_ref_table(g, reps=10):
+    """Device time of every chain of the reference's table, BF16 and INT8, on the
+    library's default path (narrow chains where measured faster), with narrow
+    chains off (the fused chain kernel) and per GEMM. L2 flushed before every
+    timed call, outside its events; seeded synthetic operands of the table's
+    shapes."""
+    torch, fg = g.torch, g.fg
+    gen = torch.Generator(device=g.dev)
+    gen.manual_seed(11)
+    out = {"workload": "the reference's 10 three-stage chains (multigemm/test/test_bf16_3.c:14-48), "
+                       "one call each, L2 flushed between calls",
+           "l2": "flushed before every timed call (256 MiB write outside the events)"}
+    launches0 = fg.kernel_launches()
+    for dt in ("bf16", "int8"):
+        rows, tot = [], {"default": 0.0, "narrow_off": 0.0, "per_gemm": 0.0}
+        flops_all = bytes_all = 0.0
+        for N, K1, Ms in REF_CHAINS:
+            Ms = list(Ms)
+            Ks = [K1] + Ms[:-1]
+            if dt == "bf16":
+                tB = torch.randn(K1, N, device=g.dev, generator=gen).to(torch.bfloat16).view(torch.int16)
+                tA = [torch.randn(m, k, device=g.dev, generator=gen).div(k ** 0.5)
+                      .to(torch.bfloat16).view(torch.int16) for m, k in zip(Ms, Ks)]
+            else:
+                tB = torch.randint(-3, 4, (K1, N), device=g.dev, generator=gen).to(torch.int8)
+                tA = [torch.randint(0, 4, (m, k), device=g.dev, generator=gen).to(torch.int8)
+                      for m, k in zip(Ms, Ks)]
+            tC = torch.empty((Ms[-1], N), dtype=torch.int32 if dt == "int8" else torch.float32,
+                             device=g.dev)
+            row = {"N": N, "K1": K1, "M": Ms}
+            for path in ("default", "narrow_off", "per_gemm"):
+                fg.set_narrow("off" if path == "narrow_off" else "auto")
+                fg.set_chain_mode("per_gemm" if path == "per_gemm" else "fused")
+                try:
+                    for _ in range(3):
+                        fg.chain_dev(dt, tC, tB, N, tA, Ms, Ks)
+                    torch.cuda.synchronize(g.dev)
+                    ts = []
+                    for i in range(reps):
+                        g.flush.fill_(i & 0xFF)
+                        a = torch.cuda.Event(enable_timing=True)
+                        b = torch.cuda.Event(enable_timing=True)
+                        a.record()
+                        fg.chain_dev(dt, tC, tB, N, tA, Ms, Ks)
+                        b.record()
+                        torch.cuda.synchronize(g.dev)
+                        ts.append(a.elapsed_time(b) * 1e3)
+                    fg.sync()
+                finally:
+                    fg.set_narrow("auto")
+                    fg.set_chain_mode("fused")
+                us = sorted(ts)[reps // 2]
+                row[f"us_{path}"] = round(us, 2)
+                tot[path] += us
+            fl = sum(2.0 * N * m * k for m, k in zip(Ms, Ks))
+            elt = 2 if dt == "bf16" else 1
+            by = K1 * N * elt + Ms[-1] * N * 4 + sum(m * k * elt for m, k in zip(Ms, Ks))
+            flops_all += fl
+            bytes_all += by
+            rows.append(row)
+        out[dt] = {
+            "chains": rows,
+            "total_us": {k: round(v, 1) for k, v in tot.items()},
+            "tflops_default": flops_all / (tot["default"] * 1e-6) / 1e12,
+            "gbs_default": bytes_all / (tot["default"] * 1e-6) / 1e9,
+            "default_vs_narrow_off": tot["narrow_off"] / tot["default"],
+            "default_vs_per_gemm": tot["per_gemm"] / tot["default"],
+        }
+    out["gpu_launches"] = fg.kernel_launches() - launches0
+    return out
+
+
 def measure_peaks(g, iters=20):
     """cuBLAS bursts at 8192^3 on this device in this run (torch): BF16, INT8
     (torch._int_mm), TF32 and plain FP32 (TF32 off) - the denominators of the
@@ -1348,7 +1430,7 @@ def main():
                     help="untimed steps (default 10; f32-groups 3)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="all",
-                    choices=["all"] + list(WORKLOADS) + ["f32-groups", "serve"],
+                    choices=["all"] + list(WORKLOADS) + ["f32-groups", "serve", "ref-chains"],
                     help="all (default): the BF16 chain as the headline line, with the INT8 "
                          "chain, the FP32 SGEMM, a grouped FP32 subset and a serving point as "
                          "sub-objects of the same line")
@@ -1399,6 +1481,9 @@ def main():
             line = run_groups(args, world, rank, local_rank)
         elif args.workload == "serve":
             line = run_serve(args, world, rank, local_rank)
+        elif args.workload == "ref-chains":
+            line = {"impl": "reference", "unavailable": "the chain table is a sub-object of the "
+                    "default line; its reference CPU timing is the chain workloads' cpu_baseline"}
         else:
             line = reference_line(args, "bf16-chain" if combined else args.workload)
         print(json.dumps(line), flush=True)
@@ -1409,6 +1494,8 @@ def main():
         line = run_groups(args, world, rank, local_rank, g)
     elif args.workload == "serve":
         line = run_serve(args, world, rank, local_rank, g)
+    elif args.workload == "ref-chains":
+        line = run_ref_table(g)
     elif not combined:
         line = run_chain_bench(args, g, args.workload)
     else:
@@ -1421,6 +1508,7 @@ def main():
         gargs.steps, gargs.warmup = min(args.steps, 20), 3
         subs["f32_groups"] = run_groups(gargs, world, rank, local_rank, g)
         subs["serve"] = run_serve(args, world, rank, local_rank, g)
+        subs["ref_chains"] = run_ref_table(g)
         if rank == 0:
             for k, v in subs.items():
                 line[k] = {kk: vv for kk, vv in v.items() if kk not in _SUB_DROP}
