@@ -199,6 +199,7 @@ struct alignas(64) NarrowArgs {
     // boxes, then the first stage's activation boxes), xslots operand buffers
     // of x_bytes (1: one column block in flight, 2: two), smem bytes in all
     int ring, slot_bytes, ra, x_bytes, xslots, smem;
+    int epi_warps;       // 4 or 8 epilogue warps
     int *status;
     // optional (else null): kNarrowTraceFields %globaltimer stamps per (CTA, unit)
     unsigned long long *trace;

@@ -19,7 +19,7 @@
 // rows runs several row tiles over the same operand. Two column blocks are in
 // flight per CTA (two operand buffers), their stages interleaved so that one
 // block's MMAs run while the other's epilogue converts. Warp 0 is the TMA
-// producer, warp 1 allocates TMEM and issues MMAs, warps 2-5 run the
+// producer, warp 1 allocates TMEM and issues MMAs, warps 2-9 run the
 // epilogues. Every wait is bounded (fg_ptx.cuh). A CTA owns its column blocks
 // entirely, so no CTA waits on another.
 #include <cuda.h>
@@ -65,14 +65,19 @@ struct NarrowGeo {
 // activation boxes they share), the operand buffers (one or two blocks in
 // flight), the output staging, the INT8 tail quad, the barriers.
 constexpr int kNQuadBytes = 4 * kNBN;
-constexpr int kNFixedBytes = kEpiStagingBytes + kNQuadBytes + 256 + 1024;
+// Epilogue warps per launch: 4 (one per TMEM lane quarter, all 128 columns) or
+// 8 (two per quarter, 64 columns each: half the work per warp, but 32 KB more
+// staging, so a smaller ring)
+__host__ __device__ constexpr int n_threads(int ew) { return 64 + 32 * ew; }
+__host__ __device__ constexpr int n_staging(int ew) { return ew * 2 * kStageBufBytes; }
+__host__ __device__ constexpr int n_fixed(int ew) { return n_staging(ew) + kNQuadBytes + 256 + 1024; }
 constexpr int kNMaxSmem = 232448;
 
 struct __align__(8) NarrowBars {
     uint64_t wfull[kNarrowMaxRing], wempty[kNarrowMaxRing];  // ring
     uint64_t xready[2];                      // operand buffer holds the next stage's input
     uint64_t acc_full[kNAcc], acc_empty[kNAcc];
-    uint64_t epi_sync;                       // the 4 epilogue warps meet (INT8 tails)
+    uint64_t epi_sync;                       // the epilogue warps meet (INT8 tails)
     uint64_t mma_done;
     uint32_t tmem_base;
     int abort;
@@ -92,7 +97,7 @@ __device__ __forceinline__ bool n_aborted(NarrowBars *b) { return *reinterpret_c
 struct NarrowWalk {
     const NarrowArgs *g;
     int nblk, step;
-    int pos[2], stage[2], row[2];
+    int pos0, pos1, stage0, stage1, row0, row1;  // per slot (plain fields: registers)
     int turn;
     __device__ void init(const NarrowArgs &args)
     {
@@ -101,9 +106,9 @@ struct NarrowWalk {
                    ? (args.nblocks - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x
                    : 0;
         step = args.xslots;
-        pos[0] = 0;
-        pos[1] = args.xslots == 2 ? 1 : (1 << 30);
-        stage[0] = stage[1] = row[0] = row[1] = 0;
+        pos0 = 0;
+        pos1 = args.xslots == 2 ? 1 : (1 << 30);
+        stage0 = stage1 = row0 = row1 = 0;
         turn = 0;
     }
     __device__ int block_of(int j) const { return (int)blockIdx.x + j * (int)gridDim.x; }
@@ -112,12 +117,13 @@ struct NarrowWalk {
     __device__ bool next(int &slot, int &j, int &st, int &r0, int &nt)
     {
         int s = turn;
-        if (pos[s] >= nblk) s ^= 1;
-        if (pos[s] >= nblk) return false;
+        if ((s ? pos1 : pos0) >= nblk) s ^= 1;
+        int pos = s ? pos1 : pos0, stage = s ? stage1 : stage0, row = s ? row1 : row0;
+        if (pos >= nblk) return false;
         slot = s;
-        j = pos[s];
-        st = stage[s];
-        r0 = row[s];
+        j = pos;
+        st = stage;
+        r0 = row;
         const int R = row_tiles(g->st[st].M);
         bool done_stage;
         if (st + 1 < g->n) {
@@ -125,14 +131,23 @@ struct NarrowWalk {
             done_stage = true;
         } else {
             nt = 1;
-            done_stage = ++row[s] == R;
+            done_stage = ++row == R;
         }
         if (done_stage) {
-            row[s] = 0;
-            if (++stage[s] == g->n) {
-                stage[s] = 0;
-                pos[s] += step;
+            row = 0;
+            if (++stage == g->n) {
+                stage = 0;
+                pos += step;
             }
+        }
+        if (s) {
+            pos1 = pos;
+            stage1 = stage;
+            row1 = row;
+        } else {
+            pos0 = pos;
+            stage0 = stage;
+            row0 = row;
         }
         turn = s ^ 1;
         return true;
@@ -172,9 +187,12 @@ __device__ __forceinline__ bool epi_meet(NarrowBars *bars, uint32_t &ph, int lan
 
 }  // namespace
 
-template <int OP>
-__global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_constant__ NarrowArgs g)
+template <int OP, int EW>
+__global__ void __launch_bounds__(n_threads(EW), 1) tc_narrow_kernel(const __grid_constant__ NarrowArgs g)
 {
+    constexpr int kNStagingBytes = n_staging(EW);
+    constexpr int kNEpiWarps = EW;
+    constexpr int CPW = (kNBN / 32) / (EW / 4);  // 32-column chunks per epilogue warp
     using G = NarrowGeo<OP>;
     constexpr MmaKind KIND = OP == OP_BF16 ? MmaKind::F16 : MmaKind::I8;
     extern __shared__ uint8_t smem_raw[];
@@ -183,8 +201,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
     uint8_t *ring = smem;                                   // slot r at r * slot_bytes
     uint8_t *xbuf = ring + g.ring * g.slot_bytes;           // operand s at s * x_bytes
     uint8_t *stg0 = xbuf + g.xslots * g.x_bytes;
-    uint32_t *quad = reinterpret_cast<uint32_t *>(stg0 + kEpiStagingBytes);
-    NarrowBars *bars = reinterpret_cast<NarrowBars *>(stg0 + kEpiStagingBytes + kNQuadBytes);
+    uint32_t *quad = reinterpret_cast<uint32_t *>(stg0 + kNStagingBytes);
+    NarrowBars *bars = reinterpret_cast<NarrowBars *>(stg0 + kNStagingBytes + kNQuadBytes);
     int *status = g.status;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -195,12 +213,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
             mbar_init(&bars->wfull[r], 1);
             mbar_init(&bars->wempty[r], 1);
         }
-        for (int s = 0; s < 2; ++s) mbar_init(&bars->xready[s], 4);
+        for (int s = 0; s < 2; ++s) mbar_init(&bars->xready[s], kNEpiWarps);
         for (int a = 0; a < kNAcc; ++a) {
             mbar_init(&bars->acc_full[a], 1);
-            mbar_init(&bars->acc_empty[a], 4);
+            mbar_init(&bars->acc_empty[a], kNEpiWarps);
         }
-        mbar_init(&bars->epi_sync, 4);
+        mbar_init(&bars->epi_sync, kNEpiWarps);
         mbar_init(&bars->mma_done, 1);
         bars->abort = 0;
         fence_mbar_init();
@@ -342,9 +360,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
             mbar_wait(&bars->mma_done, 0, status, KERR_WAIT_FULL);
         }
     } else {
-        // ------------------------------------------------------------ epilogues (warps 2..5)
-        const int quarter = warp & 3;
-        const int et = threadIdx.x - 64;  // 0..127: this thread's column for the tail quad
+        // ------------------------------------------------------------ epilogues (warps 2..9)
+        const int quarter = warp & 3;                 // TMEM lanes this warp may read
+        const int c_lo = ((warp - 2) >> 2) * CPW;     // its first 32-column chunk
+        const bool lead = quarter == 0 && c_lo == 0;  // the warp that stamps the trace
+        const int et = threadIdx.x - 64;  // 0..255: below kNBN, this thread's column for the tail quad
         uint8_t *staging = stg0 + (warp - 2) * 2 * kStageBufBytes;
         int sbuf = 0;
         unsigned tiles = 0;
@@ -360,7 +380,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
             // the first stage's input quad comes from global memory: load it
             // before waiting for the accumulators, so the two latencies overlap
             uint32_t qv0 = 0;
-            if (tails && st == 0 && n0 + et < g.N) {
+            if (tails && st == 0 && et < kNBN && n0 + et < g.N) {
                 const uint8_t *b = static_cast<const uint8_t *>(g.b);
                 for (int q = 0; q < 4 && q < cs.K; ++q)
                     qv0 |= (uint32_t)b[(size_t)q * g.ldb + n0 + et] << (8 * q);
@@ -373,14 +393,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
             }
             if (!ok) break;
             tc_fence_after();
-            if (g.trace && quarter == 0 && lane == 0) ntrace(g, u, NT_EPI_START, globaltimer_ns());
+            if (g.trace && lead && lane == 0) ntrace(g, u, NT_EPI_START, globaltimer_ns());
             // INT8 tail rows add weight quad 0 x input quad 0: the input's first
             // four rows of this block's columns, copied aside first (a later stage's
             // input is the operand buffer this unit overwrites); every warp passes
             // the meeting points alike
             if (tails) {
                 if (!(ok = epi_meet(bars, meet_ph, lane, status))) break;
-                quad[et] = st > 0 ? *reinterpret_cast<const uint32_t *>(xs + kmaj<1>(0, et)) : qv0;
+                if (et < kNBN)
+                    quad[et] = st > 0 ? *reinterpret_cast<const uint32_t *>(xs + kmaj<1>(0, et)) : qv0;
                 if (!(ok = epi_meet(bars, meet_ph, lane, status))) break;
             }
             // rows of the next stage's operand that its MMAs read (k-blocks of BK)
@@ -402,18 +423,18 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
                 // the k-block end, zeros past M (a stale NaN x 0 would be NaN)
                 bool rows_out = warp_row0 < (last ? cs.out_rows : OP == OP_I8 ? cs.M : xrows);
                 if (OP == OP_BF16 && !last && rows_out && warp_row0 >= cs.M) {
-                    // a warp wholly past M: its 32 rows of every column are zero
+                    // a warp wholly past M: its 32 rows of its columns are zero
                     const int kb = warp_row0 / G::BK, c0 = (warp_row0 % G::BK) / 8;
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        const int idx = lane + 32 * i, n = idx >> 2, c = c0 + (idx & 3);
+                    for (int i = 0; i < 4 * CPW; ++i) {
+                        const int idx = lane + 32 * i, n = c_lo * 32 + (idx >> 2), c = c0 + (idx & 3);
                         *reinterpret_cast<uint4 *>(xs + kb * kNKbBytes + n * 128 + ((c ^ (n & 7)) << 4)) =
                             make_uint4(0u, 0u, 0u, 0u);
                     }
                     rows_out = false;
                 }
 #pragma unroll 1
-                for (int c = 0; c < kNBN / 32 && rows_out; ++c) {
+                for (int c = c_lo; c < c_lo + CPW && rows_out; ++c) {
                     const int lc = c * 32, nc = n0 + lc;
                     if (nc >= g.N) break;  // warp-uniform
                     uint32_t v[32];
@@ -484,7 +505,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_narrow_kernel(const __grid_con
                 if (lane == 0) mbar_arrive(&bars->acc_empty[tt % kNAcc]);
             }
             tiles += nt;
-            if (g.trace && quarter == 0 && lane == 0) ntrace(g, u, NT_EPI_END, globaltimer_ns());
+            if (g.trace && lead && lane == 0) ntrace(g, u, NT_EPI_END, globaltimer_ns());
             if (!last) {
                 // the next stage's input is in place: tell the MMA warp
                 fence_proxy_async_smem();
@@ -541,6 +562,10 @@ namespace {
 // (row tiles of the widest intermediate) and the first stage's activations per
 // ring slot; operand buffers as deep as the widest intermediate; two column
 // blocks in flight when that leaves at least three ring slots, else one.
+// Eight epilogue warps where every intermediate is one row tile (measured on
+// the reference's chain table: INT8 N = 65536 56 -> 48 us, BF16 44 -> 40 us),
+// four where a two-tile unit needs the ring's room (eight there cost a ring slot
+// and up to 16 %).
 template <int OP>
 bool narrow_layout(const StageArgs *st, int n, NarrowArgs &A)
 {
@@ -551,15 +576,17 @@ bool narrow_layout(const StageArgs *st, int n, NarrowArgs &A)
         xkb = std::max(xkb, (st[i].M + G::BK - 1) / G::BK);
     }
     A.ra = ra;
+    A.epi_warps = ra == 1 ? 8 : 4;
     A.slot_bytes = ra * kNABytes + G::B_BYTES;
     A.x_bytes = xkb * kNKbBytes;
+    const int fixed = n_fixed(A.epi_warps);
     for (int xs = 2; xs >= 1; --xs) {
-        const int avail = kNMaxSmem - kNFixedBytes - xs * A.x_bytes;
+        const int avail = kNMaxSmem - fixed - xs * A.x_bytes;
         const int ring = std::min(kNarrowMaxRing, avail / A.slot_bytes);
         if (ring >= (xs == 2 ? 3 : 2)) {
             A.ring = ring;
             A.xslots = xs;
-            A.smem = ring * A.slot_bytes + xs * A.x_bytes + kNFixedBytes;
+            A.smem = ring * A.slot_bytes + xs * A.x_bytes + fixed;
             return true;
         }
     }
@@ -575,8 +602,11 @@ cudaError_t narrow_attr(int smem)
     int dev = 0;
     cudaGetDevice(&dev);
     if (done[dev & 63] >= smem) return cudaSuccess;
-    const cudaError_t e = cudaFuncSetAttribute(tc_narrow_kernel<OP>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, kNMaxSmem);
+    cudaError_t e = cudaFuncSetAttribute(tc_narrow_kernel<OP, 4>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kNMaxSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(tc_narrow_kernel<OP, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kNMaxSmem);
     if (e != cudaSuccess) return e;
     done[dev & 63] = kNMaxSmem;
     return cudaSuccess;
@@ -683,10 +713,17 @@ int narrow_units_per_cta(const NarrowArgs &P, int grid)
 cudaError_t launch_narrow(NarrowArgs &P, int grid, int *status, cudaStream_t s)
 {
     P.status = status;
-    if (P.op == OP_BF16)
-        tc_narrow_kernel<OP_BF16><<<grid, kThreads, P.smem, s>>>(P);
-    else
-        tc_narrow_kernel<OP_I8><<<grid, kThreads, P.smem, s>>>(P);
+    if (P.op == OP_BF16) {
+        if (P.epi_warps == 8)
+            tc_narrow_kernel<OP_BF16, 8><<<grid, n_threads(8), P.smem, s>>>(P);
+        else
+            tc_narrow_kernel<OP_BF16, 4><<<grid, n_threads(4), P.smem, s>>>(P);
+    } else {
+        if (P.epi_warps == 8)
+            tc_narrow_kernel<OP_I8, 8><<<grid, n_threads(8), P.smem, s>>>(P);
+        else
+            tc_narrow_kernel<OP_I8, 4><<<grid, n_threads(4), P.smem, s>>>(P);
+    }
     return cudaGetLastError();
 }
 
