@@ -1041,10 +1041,22 @@ int host_chain(int dtype, void *C, const void *B, long N, int n, const void *con
     }
     const size_t mark = c->arena_off;
     int chunks = 0;
+    // pageable C: each chunk leaves staging once its download has landed,
+    // between the later chunks' staging (opportunistically) or at the end
+    int copied_out = 0;
+    auto copy_out = [&](int jo) {
+        const long o0 = jo * cw, o1 = o0 + cw < N ? o0 + cw : N;
+        const size_t wo = (size_t)(o1 - o0) * out_elt;
+        c->copier->copy(static_cast<char *>(C) + o0 * out_elt, ldc * out_elt,
+                        c->pin + pin_c + (size_t)rows * o0 * out_elt, wo, wo, rows);
+    };
     for (int j = 0; j < nchunk; ++j) {
         const long c0 = j * cw, c1 = c0 + cw < N ? c0 + cw : N;
         if (c0 >= N) break;
         ++chunks;
+        if (mc == HostMem::Pageable && rows > 0)
+            while (copied_out < j && cudaEventQuery(c->ev_down[copied_out]) == cudaSuccess)
+                copy_out(copied_out++);
         const size_t wb = (size_t)(c1 - c0) * elt;
         char *bj = static_cast<char *>(bd) + c0 * elt;
         char *cj = static_cast<char *>(cd) + c0 * out_elt;
@@ -1087,17 +1099,14 @@ int host_chain(int dtype, void *C, const void *B, long N, int n, const void *con
         }
     }
     if (mc == HostMem::Pageable && rows > 0) {
-        // each chunk of C leaves staging as soon as it has arrived
-        for (int j = 0; j < chunks; ++j) {
-            const long c0 = j * cw, c1 = c0 + cw < N ? c0 + cw : N;
+        // the chunks of C not yet out of staging, each as soon as it has arrived
+        for (int j = copied_out; j < chunks; ++j) {
             const cudaError_t e = cudaEventSynchronize(c->ev_down[j]);
             if (e != cudaSuccess) {
                 drain();
                 return fail(FG_ERR_CUDA, "chain download: %s", cudaGetErrorString(e));
             }
-            const size_t wc = (size_t)(c1 - c0) * out_elt;
-            c->copier->copy(static_cast<char *>(C) + c0 * out_elt, ldc * out_elt,
-                            c->pin + pin_c + (size_t)rows * c0 * out_elt, wc, wc, rows);
+            copy_out(j);
         }
     }
     CUDA_TRY(cudaStreamSynchronize(c->stream_d2h));
