@@ -385,6 +385,16 @@ __global__ void __launch_bounds__(n_threads(EW), 1) tc_narrow_kernel(const __gri
                 for (int q = 0; q < 4 && q < cs.K; ++q)
                     qv0 |= (uint32_t)b[(size_t)q * g.ldb + n0 + et] << (8 * q);
             }
+            // likewise this lane's weight quad 0 of each tail row of the unit
+            uint32_t wq_t[2] = {0u, 0u};
+            if (tails)
+#pragma unroll
+                for (int t = 0; t < 2; ++t) {
+                    const int row = (r0 + t) * 128 + quarter * 32 + lane;
+                    if (t < nt && row >= cs.tail_lo && row < cs.tail_hi)
+                        wq_t[t] = *reinterpret_cast<const uint32_t *>(
+                            cs.w_tail + (size_t)(row - cs.tail_row0) * cs.ld_w_tail + cs.K);
+                }
             // every tile of the unit: an intermediate overwrites the operand they read
             for (int t = 0; t < nt && ok; ++t) {
                 const unsigned tt = tiles + t;
@@ -413,10 +423,7 @@ __global__ void __launch_bounds__(n_threads(EW), 1) tc_narrow_kernel(const __gri
                 const uint32_t t_row =
                     tmem_base + (tt % kNAcc) * kNBN + ((uint32_t)(quarter * 32) << 16);
                 const bool tail_row = tails && row >= cs.tail_lo && row < cs.tail_hi;
-                uint32_t wq = 0;
-                if (tail_row)
-                    wq = *reinterpret_cast<const uint32_t *>(
-                        cs.w_tail + (size_t)(row - cs.tail_row0) * cs.ld_w_tail + cs.K);
+                const uint32_t wq = t == 0 ? wq_t[0] : wq_t[1];
                 // rows written: the result's stored rows; an INT8 intermediate's M
                 // rows (the next stage's weights are zero past its K = M, and
                 // 0 x anything is 0 in integers); a BF16 intermediate's rows up to
@@ -441,13 +448,15 @@ __global__ void __launch_bounds__(n_threads(EW), 1) tc_narrow_kernel(const __gri
                     tmem_ld_32x32b_x32(t_row + c * 32, v);
                     tmem_ld_wait();
                     if (tail_row) {
+                        // + sum over q of weight byte q (unsigned) x input byte q
+                        // (signed): one mixed-sign dp4a per value, exact in int32
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const int a = (int)((wq >> (8 * q)) & 0xffu);
-#pragma unroll
-                            for (int jj = 0; jj < 32; ++jj)
-                                v[jj] = (uint32_t)((int32_t)v[jj] +
-                                                   a * (int)(int8_t)((quad[lc + jj] >> (8 * q)) & 0xffu));
+                        for (int jj = 0; jj < 32; ++jj) {
+                            int r;
+                            asm("dp4a.u32.s32 %0, %1, %2, %3;"
+                                : "=r"(r)
+                                : "r"(wq), "r"(quad[lc + jj]), "r"((int)v[jj]));
+                            v[jj] = (uint32_t)r;
                         }
                     }
                     if (last) {
