@@ -396,17 +396,26 @@ __device__ __forceinline__ void stage_chunk(const StageArgs &p, uint8_t *sb, int
     }
 }
 
-// INT8 reference tail rows: add back weight quad 0 x activation quad 0.
-__device__ __forceinline__ void tail_fix(const StageArgs &p, uint32_t wq, int nc, uint32_t (&v)[32])
+// INT8 reference tail rows: add back weight quad 0 x activation quad 0. The
+// whole warp takes part (it loads each column's input quad once, lane l column
+// nc + l, and passes it round); lanes of tail rows add it with one mixed-sign
+// dp4a (weight bytes unsigned, input bytes signed), exact in int32.
+__device__ __forceinline__ void tail_fix(const StageArgs &p, uint32_t wq, bool tail, int nc, int lane,
+                                         uint32_t (&v)[32])
 {
-    const int8_t *x = reinterpret_cast<const int8_t *>(p.x);
+    const uint8_t *x = reinterpret_cast<const uint8_t *>(p.x);
+    uint32_t qp = 0;
+    if (nc + lane < p.N)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int a = (int)((wq >> (8 * q)) & 0xffu);
-        const int8_t *xr = x + (size_t)q * p.ld_x + nc;
+        for (int q = 0; q < 4; ++q) qp |= (uint32_t)x[(size_t)q * p.ld_x + nc + lane] << (8 * q);
 #pragma unroll
-        for (int j = 0; j < 32; ++j)
-            if (nc + j < p.N) v[j] = (uint32_t)((int32_t)v[j] + a * (int32_t)xr[j]);
+    for (int j = 0; j < 32; ++j) {
+        const uint32_t qj = __shfl_sync(0xffffffffu, qp, j);
+        if (tail && nc + j < p.N) {
+            int r;
+            asm("dp4a.u32.s32 %0, %1, %2, %3;" : "=r"(r) : "r"(wq), "r"(qj), "r"((int)v[j]));
+            v[j] = (uint32_t)r;
+        }
     }
 }
 
@@ -424,6 +433,7 @@ __device__ __forceinline__ void drain_staged(const StageArgs &p, const CUtensorM
         wq = *reinterpret_cast<const uint32_t *>(reinterpret_cast<const uint8_t *>(p.w_tail) +
                                                  (size_t)(row - p.tail_row0) * p.ld_w_tail + p.K);
     const bool rows_in = warp_row0 < p.M;
+    const bool warp_tail = __any_sync(0xffffffffu, tail);
 #pragma unroll 1
     for (int b = 0; b < BN / COLS; ++b) {
         const int col0 = n0 + b * COLS;
@@ -438,11 +448,11 @@ __device__ __forceinline__ void drain_staged(const StageArgs &p, const CUtensorM
             if (CPB > 1) tmem_ld_32x32b_x32(t_row + (b * CPB + cc + 1) * 32, vb);
             tmem_ld_wait();
             const int nca = col0 + cc * 32;
-            if (tail) tail_fix(p, wq, nca, va);
+            if (warp_tail) tail_fix(p, wq, tail, nca, lane, va);
             stage_chunk<EPI>(p, sb, lane, row, cc * 32, nca + 32 <= p.N, va);
             if (CPB > 1) {
                 const int ncb = nca + 32;
-                if (tail) tail_fix(p, wq, ncb, vb);
+                if (warp_tail) tail_fix(p, wq, tail, ncb, lane, vb);
                 stage_chunk<EPI>(p, sb, lane, row, (cc + 1) * 32, ncb + 32 <= p.N, vb);
             }
         }
