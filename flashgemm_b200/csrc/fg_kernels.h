@@ -175,6 +175,7 @@ cudaError_t launch_single_group(const GroupLaunch &g, const void *tables_dev, in
 constexpr int kNarrowRows = 256;
 constexpr int kNarrowMaxStages = 8;
 constexpr int kNarrowMaxRing = 4;
+constexpr int kNarrowMaxX = 4;       // column blocks in flight per CTA, at most
 
 struct alignas(64) NarrowStage {
     CUtensorMap tm_w;    // weights, K-major boxes of 128 rows x 128 bytes
@@ -197,7 +198,7 @@ struct alignas(64) NarrowArgs {
     int op;              // OperandKind
     // shared memory layout of the launch: ring slots of slot_bytes (ra weight
     // boxes, then the first stage's activation boxes), xslots operand buffers
-    // of x_bytes (1: one column block in flight, 2: two), smem bytes in all
+    // of x_bytes (one per column block in flight, 1 to kNarrowMaxX), smem bytes in all
     int ring, slot_bytes, ra, x_bytes, xslots, smem;
     int epi_warps;       // 4 or 8 epilogue warps
     int *status;

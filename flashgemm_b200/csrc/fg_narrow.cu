@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -75,7 +76,7 @@ constexpr int kNMaxSmem = 232448;
 
 struct __align__(8) NarrowBars {
     uint64_t wfull[kNarrowMaxRing], wempty[kNarrowMaxRing];  // ring
-    uint64_t xready[2];                      // operand buffer holds the next stage's input
+    uint64_t xready[kNarrowMaxX];            // operand buffer holds the next stage's input
     uint64_t acc_full[kNAcc], acc_empty[kNAcc];
     uint64_t epi_sync;                       // the epilogue warps meet (INT8 tails)
     uint64_t mma_done;
@@ -88,16 +89,18 @@ __device__ __forceinline__ void n_set_abort(NarrowBars *b) { *reinterpret_cast<v
 __device__ __forceinline__ bool n_aborted(NarrowBars *b) { return *reinterpret_cast<volatile int *>(&b->abort) != 0; }
 
 // The work units of one CTA in the order every role walks them. The CTA owns
-// column blocks cta, cta + grid, ...; with two operand buffers they alternate
-// between them (slot = position % 2) and the units of the two slots' current
+// column blocks cta, cta + grid, ...; with X operand buffers (1 to 4) they take
+// turns between them (slot = position % X) and the units of the slots' current
 // blocks interleave. A unit is a whole intermediate stage (all its row tiles:
 // its epilogue overwrites the operand those tiles read, so it waits for all of
 // them, and they share each k-block of their B operand) or one row tile of the
 // last stage (written to global memory).
 struct NarrowWalk {
     const NarrowArgs *g;
-    int nblk, step;
-    int pos0, pos1, stage0, stage1, row0, row1;  // per slot (plain fields: registers)
+    int nblk, xs;
+    // per operand buffer s: block position, stage and row tile of its next unit
+    // (plain fields, selected by switch: they stay in registers)
+    int p0, p1, p2, p3, st0, st1, st2, st3, rw0, rw1, rw2, rw3;
     int turn;
     __device__ void init(const NarrowArgs &args)
     {
@@ -105,21 +108,27 @@ struct NarrowWalk {
         nblk = (int)blockIdx.x < args.nblocks
                    ? (args.nblocks - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x
                    : 0;
-        step = args.xslots;
-        pos0 = 0;
-        pos1 = args.xslots == 2 ? 1 : (1 << 30);
-        stage0 = stage1 = row0 = row1 = 0;
+        xs = args.xslots;
+        p0 = 0;
+        p1 = xs > 1 ? 1 : (1 << 30);
+        p2 = xs > 2 ? 2 : (1 << 30);
+        p3 = xs > 3 ? 3 : (1 << 30);
+        st0 = st1 = st2 = st3 = rw0 = rw1 = rw2 = rw3 = 0;
         turn = 0;
     }
     __device__ int block_of(int j) const { return (int)blockIdx.x + j * (int)gridDim.x; }
     __device__ static int row_tiles(int M) { return (M + 127) / 128; }
-    // Next unit: slot, block position j, stage, first row tile, row tiles.
+    __device__ int pos_of(int s) const { return s == 0 ? p0 : s == 1 ? p1 : s == 2 ? p2 : p3; }
+    // Next unit: slot, block position j, stage, first row tile, row tiles; the
+    // buffers take turns, a buffer whose blocks are done drops out.
     __device__ bool next(int &slot, int &j, int &st, int &r0, int &nt)
     {
         int s = turn;
-        if ((s ? pos1 : pos0) >= nblk) s ^= 1;
-        int pos = s ? pos1 : pos0, stage = s ? stage1 : stage0, row = s ? row1 : row0;
+        for (int k = 0; k < 4 && pos_of(s) >= nblk; ++k) s = s + 1 < xs ? s + 1 : 0;
+        int pos = pos_of(s);
         if (pos >= nblk) return false;
+        int stage = s == 0 ? st0 : s == 1 ? st1 : s == 2 ? st2 : st3;
+        int row = s == 0 ? rw0 : s == 1 ? rw1 : s == 2 ? rw2 : rw3;
         slot = s;
         j = pos;
         st = stage;
@@ -137,19 +146,16 @@ struct NarrowWalk {
             row = 0;
             if (++stage == g->n) {
                 stage = 0;
-                pos += step;
+                pos += xs;
             }
         }
-        if (s) {
-            pos1 = pos;
-            stage1 = stage;
-            row1 = row;
-        } else {
-            pos0 = pos;
-            stage0 = stage;
-            row0 = row;
+        switch (s) {
+        case 0: p0 = pos; st0 = stage; rw0 = row; break;
+        case 1: p1 = pos; st1 = stage; rw1 = row; break;
+        case 2: p2 = pos; st2 = stage; rw2 = row; break;
+        default: p3 = pos; st3 = stage; rw3 = row; break;
         }
-        turn = s ^ 1;
+        turn = s + 1 < xs ? s + 1 : 0;
         return true;
     }
 };
@@ -213,7 +219,7 @@ __global__ void __launch_bounds__(n_threads(EW), 1) tc_narrow_kernel(const __gri
             mbar_init(&bars->wfull[r], 1);
             mbar_init(&bars->wempty[r], 1);
         }
-        for (int s = 0; s < 2; ++s) mbar_init(&bars->xready[s], kNEpiWarps);
+        for (int s = 0; s < kNarrowMaxX; ++s) mbar_init(&bars->xready[s], kNEpiWarps);
         for (int a = 0; a < kNAcc; ++a) {
             mbar_init(&bars->acc_full[a], 1);
             mbar_init(&bars->acc_empty[a], kNEpiWarps);
@@ -293,18 +299,18 @@ __global__ void __launch_bounds__(n_threads(EW), 1) tc_narrow_kernel(const __gri
             int r = 0;
             uint32_t rph = 0;
             unsigned tiles = 0;      // tiles issued: accumulator tiles % kNAcc, phase (tiles / kNAcc) & 1
-            int xr[2] = {0, 0};      // stage inputs consumed per slot: the xready phase
+            uint32_t xr = 0;         // bit s: the xready phase to wait for on buffer s
             int slot, j, st, r0, nt;
             for (int u = 0; walk.next(slot, j, st, r0, nt); ++u) {
                 const NarrowStage &cs = g.st[st];
                 if (g.trace) ntrace(g, u, NT_MMA_WAIT, globaltimer_ns());
                 if (st > 0 && r0 == 0) {
-                    if (!mbar_wait(&bars->xready[slot], (uint32_t)(xr[slot] & 1), status,
+                    if (!mbar_wait(&bars->xready[slot], (xr >> slot) & 1u, status,
                                    KERR_WAIT_FULL)) {
                         n_set_abort(bars);
                         goto mma_done;
                     }
-                    ++xr[slot];
+                    xr ^= 1u << slot;
                     tc_fence_after();
                 }
                 for (int t = 0; t < nt; ++t) {  // the unit's accumulators
@@ -589,7 +595,15 @@ bool narrow_layout(const StageArgs *st, int n, NarrowArgs &A)
     A.slot_bytes = ra * kNABytes + G::B_BYTES;
     A.x_bytes = xkb * kNKbBytes;
     const int fixed = n_fixed(A.epi_warps);
-    for (int xs = 2; xs >= 1; --xs) {
+    // at most two column blocks in flight (FG_NARROW_XSLOTS=<1..4> overrides):
+    // four measured slower on the reference's table (INT8 409 against 389 us,
+    // BF16 389 against 383), their smaller ring outweighing the extra overlap
+    static const int max_xs = [] {
+        const char *v = getenv("FG_NARROW_XSLOTS");
+        const int x = v ? atoi(v) : 2;
+        return x < 1 ? 1 : x > kNarrowMaxX ? kNarrowMaxX : x;
+    }();
+    for (int xs = max_xs; xs >= 1; --xs) {
         const int avail = kNMaxSmem - fixed - xs * A.x_bytes;
         const int ring = std::min(kNarrowMaxRing, avail / A.slot_bytes);
         if (ring >= (xs == 2 ? 3 : 2)) {
