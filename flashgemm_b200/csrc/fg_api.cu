@@ -549,12 +549,15 @@ int build_tc_stages(DevCtx *c, int dtype, int sem, void *C, long ldc, Mat b, lon
             const void *wmain = pw ? pw[i].w : a[i].p;
             long ldmain = pw ? pw[i].ld : a[i].ld;
             if ((ldmain % 16) || !aligned16(wmain)) {
+                // a padded copy: a job of the same batched launch as the tail blocks
                 uint8_t *wp = (uint8_t *)take((size_t)Mi * ldw);
-                int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 weight copy", [&] {
-                    return launch_prep_int8_weights((const int8_t *)a[i].p, a[i].ld, wp, ldw, Mi,
-                                                    Ki, 0, 0, c->work);
-                });
-                if (st) return st;
+                if (jobs.n == 8) {  // flush a full batch
+                    int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 weight prep",
+                                        [&] { return launch_prep_int8_jobs(jobs, c->work); });
+                    if (st) return st;
+                    jobs.n = 0;
+                }
+                jobs.job[jobs.n++] = PrepJob{(const int8_t *)a[i].p, a[i].ld, wp, ldw, Mi, Ki, 0, 0};
                 wmain = wp;
                 ldmain = ldw;
             }
@@ -569,7 +572,7 @@ int build_tc_stages(DevCtx *c, int dtype, int sem, void *C, long ldc, Mat b, lon
                 const long row0 = (tail_lo / 256) * 256;
                 uint8_t *wt = (uint8_t *)take((size_t)(Mi - row0) * ldw);
                 if (jobs.n == 8) {  // flush a full batch
-                    int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 tail-row prep",
+                    int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 weight prep",
                                         [&] { return launch_prep_int8_jobs(jobs, c->work); });
                     if (st) return st;
                     jobs.n = 0;
@@ -596,8 +599,8 @@ int build_tc_stages(DevCtx *c, int dtype, int sem, void *C, long ldc, Mat b, lon
             x = s.out;
             ldx = s.ld_out;
         }
-        if (jobs.n) {  // all tail blocks of the chain in one launch
-            int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 tail-row prep",
+        if (jobs.n) {  // the chain's padded copies and tail blocks in one launch
+            int st = run_kernel(c, FG_PK_AUX, 0.0, "int8 weight prep",
                                 [&] { return launch_prep_int8_jobs(jobs, c->work); });
             if (st) return st;
         }
