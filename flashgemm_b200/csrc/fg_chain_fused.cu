@@ -29,6 +29,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <iterator>
@@ -566,15 +567,36 @@ int window_blocks()
 }
 
 // FG_CHAIN_FEED=0: no feeder workers (see SchedOpts) in a single chain's schedule;
-// otherwise the host tries them at every streamed boundary and keeps them when
-// the estimate is at least 1 % shorter.
+// FG_CHAIN_FEED=<stage>,<pairs>,<rows>: exactly those feeders (when that stage's
+// boundary streams); otherwise the host tries them at every streamed boundary and
+// keeps them when the estimate is at least 1 % shorter.
 bool feed_mode()
 {
     static const bool on = [] {
         const char *v = getenv("FG_CHAIN_FEED");
-        return !(v && v[0] == '0');
+        return !(v && v[0] == '0' && v[1] == 0);
     }();
     return on;
+}
+bool feed_forced(SchedOpts &o)
+{
+    static const int f[3] = {-1, 0, 0};
+    static const bool forced = [] {
+        const char *v = getenv("FG_CHAIN_FEED");
+        int a = -1, b = 0, c = 0;
+        if (v && sscanf(v, "%d,%d,%d", &a, &b, &c) == 3 && a >= 0 && b > 0 && c > 0) {
+            const_cast<int *>(f)[0] = a;
+            const_cast<int *>(f)[1] = b;
+            const_cast<int *>(f)[2] = c;
+            return true;
+        }
+        return false;
+    }();
+    if (!forced) return false;
+    o.feed_stage = f[0];
+    o.feed_workers = f[1];
+    o.feed_rows = f[2];
+    return true;
 }
 
 constexpr unsigned kStreamAuto = ~0u;
@@ -707,7 +729,11 @@ static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, in
             list_schedule(ss.data(), n, pairs, 2.0, off_s, ent_s, &span_stream, nullptr, &base);
             // feeders at a streamed boundary (see SchedOpts): the best of a small grid
             SchedOpts chosen = base;
-            if (feed_mode()) {
+            SchedOpts forced = base;
+            if (feed_forced(forced) && forced.feed_stage + 1 < n && ((mask >> forced.feed_stage) & 1u)) {
+                list_schedule(ss.data(), n, pairs, 2.0, off_s, ent_s, &span_stream, nullptr, &forced);
+                chosen = forced;
+            } else if (feed_mode()) {
                 SchedOpts best = base;
                 double span_best = span_stream;
                 std::vector<int> off_f;
