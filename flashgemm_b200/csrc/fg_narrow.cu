@@ -228,6 +228,13 @@ __global__ void __launch_bounds__(n_threads(EW), 1) tc_narrow_kernel(const __gri
         mbar_init(&bars->mma_done, 1);
         bars->abort = 0;
         fence_mbar_init();
+        // the tensor maps into the TMA unit's cache before their first use
+        tma_prefetch_desc(&g.tm_b);
+        for (int i = 0; i < g.n; ++i) {
+            tma_prefetch_desc(&g.st[i].tm_w);
+            if (g.st[i].tail_hi > g.st[i].tail_lo) tma_prefetch_desc(&g.st[i].tm_wt);
+        }
+        tma_prefetch_desc(&g.st[g.n - 1].tm_out);
     }
     if (warp == 1) tmem_alloc(&bars->tmem_base, kNAcc * kNBN);
     tc_fence_before();

@@ -217,6 +217,16 @@ __global__ void __launch_bounds__(kPThreads, 1) tc_panel_kernel(const __grid_con
         mbar_init(&bars->mma_done, 1);
         bars->abort = 0;
         fence_mbar_init();
+        // the first block's chain's tensor maps into the TMA unit's cache
+        const int q0 = g.blocks ? g.off[blockIdx.x] : 0;
+        if (!g.blocks || q0 < g.off[blockIdx.x + 1]) {
+            const PanelChain &ch = chain_of(g, blk(g, q0));
+            tma_prefetch_desc(&ch.tm_b);
+            for (int i = 0; i < ch.n; ++i) {
+                tma_prefetch_desc(&ch.tm_w[i][0]);
+                tma_prefetch_desc(&ch.tm_w[i][1]);
+            }
+        }
     }
     if (warp == 1) tmem_alloc(&bars->tmem_base, kPTmemCols);
     tc_fence_before();
