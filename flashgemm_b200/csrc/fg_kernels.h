@@ -45,6 +45,7 @@ struct StageArgs {
     int tail_row0;
     int kchunk;        // TF32X3: k-blocks (of 32) per FP32 promotion of the partial sum
     int tma_store;     // set by the launchers: the epilogue writes `out` with TMA bulk stores
+    int l2_keep;       // 1: `out` is an intermediate stored with an L2 evict-last policy
     int *status;       // device status word (0 = ok)
 };
 

@@ -177,6 +177,15 @@ __device__ __forceinline__ uint64_t l2_policy_evict_first()
     return p;
 }
 
+// Evict-last: lines kept in preference to others (within the context's
+// persisting set-aside, where one is configured).
+__device__ __forceinline__ uint64_t l2_policy_evict_last()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 
 // Wait until at most N committed bulk groups of this thread still read shared memory.

@@ -461,9 +461,14 @@ __device__ __forceinline__ void drain_staged(const StageArgs &p, const CUtensorM
         if (lane == 0 && rows_in) {
             // a chain's result is not read again in the launch: first out of L2, so
             // that the intermediates the next stages read stay in it
-            if constexpr (EPI == EPI_BF16 || EPI == EPI_S8)
-                tma_store_2d(tm_out, sb, col0, warp_row0);
-            else
+            if constexpr (EPI == EPI_BF16 || EPI == EPI_S8) {
+                // an intermediate: kept in L2 where asked, so that the later stage
+                // that overwrites the buffer finds it there and it is never written back
+                if (p.l2_keep)
+                    tma_store_2d_hint(tm_out, sb, col0, warp_row0, l2_policy_evict_last());
+                else
+                    tma_store_2d(tm_out, sb, col0, warp_row0);
+            } else
                 tma_store_2d_hint(tm_out, sb, col0, warp_row0, l2_policy_evict_first());
             bulk_commit();
         }
