@@ -347,6 +347,33 @@ def test_streamed_hand_off_is_bit_identical(dt, tmp_path):
     assert_parity(dt, outs["1"], want, (Ms[-1] // 4) * 4 if dt == "int8" else None)
 
 
+def test_int8_intermediates_l2_policy_is_bit_identical(tmp_path):
+    """INT8 intermediates stored with an L2 evict-last policy (the default), with
+    plain stores (FG_L2_KEEP=0), and with an L2 set-aside for them (FG_L2_KEEP=96)
+    give identical bits: the policy only decides which lines stay in L2."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = {}
+    for mode in ("", "0", "96"):
+        path = str(tmp_path / f"c{mode or 'default'}.npy")
+        env = dict(os.environ, PYTHONPATH=os.pathsep.join([root, os.path.join(root, "oracle")]))
+        env.pop("FG_L2_KEEP", None)
+        if mode:
+            env["FG_L2_KEEP"] = mode
+        r = subprocess.run([sys.executable, "-c", _STREAM_SCRIPT, root, "int8", path], env=env,
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout + r.stderr
+        outs[mode] = np.load(path)
+    np.testing.assert_array_equal(outs[""], outs["0"])
+    np.testing.assert_array_equal(outs[""], outs["96"])
+    N, K1, Ms = 768, 256, [1000, 520, 136, 300]
+    B, As, Ks = oracle.chain_inputs("int8", N, K1, Ms, seed=43)
+    want = oracle.chain("int8", B, As, N, Ms, Ks, mode=oracle.REF, threads=1)
+    assert_parity("int8", outs[""], want, (Ms[-1] // 4) * 4)
+
+
 @pytest.mark.parametrize("dt,f32algo", [("int8", None), ("bf16", None), ("f32", "ffma"),
                                         ("f32", "3xtf32")])
 def test_registered_weights_match_per_call_weights(fg, dt, f32algo):
