@@ -780,6 +780,9 @@ def run_serve(args, world, rank, local_rank, ctx=None):
     # one that sheds requests still queued args.serve_deadline_us after submit
     plain_srv = fg.Server(max_batch=64, slots=2, max_wait_us=200)
     shed_srv = None
+    if args.serve_deadline_us > 0 and any(f > 1.0 for f in args.serve_rates):
+        shed_srv = fg.Server(max_batch=64, slots=2, max_wait_us=200,
+                             max_queue_us=args.serve_deadline_us)
     srv = plain_srv
 
     def run_point(reqs, at_us, prof=False):
@@ -810,6 +813,10 @@ def run_serve(args, world, rank, local_rank, ctx=None):
     # capacity: the better of two bursts (the loop's host side shares the CPU)
     warm = serve_requests(seed + 1, sets, min(2000, nreq))
     run_point(warm, [0.0] * len(warm))
+    if shed_srv is not None:  # the same warm-up for the server of the overload points
+        srv = shed_srv
+        run_point(warm, [0.0] * len(warm))
+        srv = plain_srv
     capacity = 0.0
     for k in range(2):
         burst = serve_requests(seed + 2 + 100 * k, sets, min(4000, nreq))
@@ -822,10 +829,7 @@ def run_serve(args, world, rank, local_rank, ctx=None):
     rng = np.random.default_rng(seed + 3)
     with sampler:
         for k, frac in enumerate(args.serve_rates):
-            if frac > 1.0 and args.serve_deadline_us > 0:
-                if shed_srv is None:
-                    shed_srv = fg.Server(max_batch=64, slots=2, max_wait_us=200,
-                                         max_queue_us=args.serve_deadline_us)
+            if frac > 1.0 and shed_srv is not None:
                 srv = shed_srv
             else:
                 srv = plain_srv
