@@ -347,6 +347,55 @@ def test_streamed_hand_off_is_bit_identical(dt, tmp_path):
     assert_parity(dt, outs["1"], want, (Ms[-1] // 4) * 4 if dt == "int8" else None)
 
 
+_PARAMS_SCRIPT = """
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import flashgemm_b200 as fg, oracle
+dt, out, N, K1 = sys.argv[2], sys.argv[3], int(sys.argv[4]), int(sys.argv[5])
+Ms = [int(m) for m in sys.argv[6].split(",")]
+B, As, Ks = oracle.chain_inputs(dt, N, K1, Ms, seed=47)
+fg.set_semantics("ref")
+C = np.zeros((Ms[-1], N), np.int32 if dt == "int8" else np.float32)
+args = []
+for a, m, k in zip(As, Ms, Ks):
+    args += [a, m, k]
+getattr(fg, {"int8": "flashgemm_multi_int8uint8int32",
+             "bf16": "flashgemm_multi_bf16bf16f32"}[dt])(C, B, N, len(Ms), *args, check=True)
+fg.sync()
+np.save(out, C)
+"""
+
+
+@pytest.mark.parametrize("dt,N,K1,Ms", [
+    ("bf16", 1024, 256, [512, 288, 512]),                       # 3 stages, few entries
+    ("int8", 768, 256, [520, 300, 264, 512, 280, 136]),         # 6 stages
+])
+def test_fused_chain_parameter_blocks_are_bit_identical(tmp_path, dt, N, K1, Ms):
+    """A fused chain launched with the largest parameter block (FG_CHAIN_PARAMS=big)
+    and with the smallest one its stages and schedule fit computes identical bits."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = {}
+    for mode in ("", "big"):
+        path = str(tmp_path / f"c{mode or 'default'}.npy")
+        env = dict(os.environ, PYTHONPATH=os.pathsep.join([root, os.path.join(root, "oracle")]))
+        env.pop("FG_CHAIN_PARAMS", None)
+        if mode:
+            env["FG_CHAIN_PARAMS"] = mode
+        r = subprocess.run([sys.executable, "-c", _PARAMS_SCRIPT, root, dt, path, str(N), str(K1),
+                            ",".join(map(str, Ms))], env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stdout + r.stderr
+        outs[mode] = np.load(path)
+    np.testing.assert_array_equal(outs[""], outs["big"])
+    B, As, Ks = oracle.chain_inputs(dt, N, K1, Ms, seed=47)
+    want = oracle.chain(dt, B, As, N, Ms, Ks, mode=oracle.REF, threads=1)
+    assert_parity(dt, outs[""], want, (Ms[-1] // 4) * 4 if dt == "int8" else None)
+
+
 def test_int8_intermediates_l2_policy_is_bit_identical(tmp_path):
     """INT8 intermediates stored with an L2 evict-last policy (the default), with
     plain stores (FG_L2_KEEP=0), and with an L2 set-aside for them (FG_L2_KEEP=96)
