@@ -184,12 +184,13 @@ int get_ctx(DevCtx **out)
         CUDA_TRY(cudaMalloc(&c->status, sizeof(int)));
         CUDA_TRY(cudaMemset(c->status, 0, sizeof(int)));
         CUDA_TRY(cudaMallocHost(&c->status_host, sizeof(int)));
-        if (l2_keep().setaside_mb > 0) {
+        if (l2_keep().setaside_mb > 0) {  // a tuning: where the device refuses it, run without
             int mx = 0;
-            CUDA_TRY(cudaDeviceGetAttribute(&mx, cudaDevAttrMaxPersistingL2CacheSize, dev));
             const size_t want = (size_t)l2_keep().setaside_mb << 20;
-            CUDA_TRY(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize,
-                                        want < (size_t)mx ? want : (size_t)mx));
+            if (cudaDeviceGetAttribute(&mx, cudaDevAttrMaxPersistingL2CacheSize, dev) != cudaSuccess ||
+                cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize,
+                                   want < (size_t)mx ? want : (size_t)mx) != cudaSuccess)
+                cudaGetLastError();
         }
         g_ctx[dev] = c;
     }

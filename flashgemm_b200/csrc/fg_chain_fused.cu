@@ -714,10 +714,16 @@ static cudaError_t launch_chain_op(const StageArgs *stages, int n, int *done, in
         }
     };
     auto set_run = [](Built *b, int *done, int *status, unsigned long long *trace) {
-        b->P.done = done, b->P.status = status, b->P.trace = trace;
-        if (b->s4t) b->s4t->done = done, b->s4t->status = status, b->s4t->trace = trace;
-        if (b->s4s) b->s4s->done = done, b->s4s->status = status, b->s4s->trace = trace;
-        if (b->s8s) b->s8s->done = done, b->s8s->status = status, b->s8s->trace = trace;
+        auto set = [&](auto *q) {
+            if (!q) return;
+            q->done = done;
+            q->status = status;
+            q->trace = trace;
+        };
+        set(&b->P);
+        set(b->s4t.get());
+        set(b->s4s.get());
+        set(b->s8s.get());
     };
     static std::vector<Built *> built;  // most recently used last, at most kBuiltKept
     constexpr size_t kBuiltKept = 8;
