@@ -93,6 +93,36 @@ def test_shape_mismatch_rejected(fg):
     assert "previous M" in fg.last_error()
 
 
+def test_noalloc_arguments_checked_before_device_work(fg):
+    """The allocation-free BF16 chain refuses bad shapes, strides and alignments on
+    the host, before any CUDA call (the addresses below are never dereferenced)."""
+    import ctypes
+    L = fg.lib()
+    f = L.fg_chain_bf16_noalloc
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long, ctypes.c_int,
+                  ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_long),
+                  ctypes.POINTER(ctypes.c_long), ctypes.c_void_p, ctypes.c_void_p]
+
+    def call(N, Ms, Ks, C=0x10000, B=0x20000, A=0x30000):
+        n = len(Ms)
+        As = (ctypes.c_void_p * n)(*[A + 0x1000 * i for i in range(n)])
+        return f(C, B, N, n, As, (ctypes.c_long * n)(*Ms), (ctypes.c_long * n)(*Ks), None, None)
+
+    cases = [
+        (dict(N=(1 << 30) + 8, Ms=[64], Ks=[64]), "2^30"),
+        (dict(N=100, Ms=[64], Ks=[64]), "multiple of 8"),
+        (dict(N=256, Ms=[64, 32], Ks=[64, 48]), "previous M"),
+        (dict(N=256, Ms=[64], Ks=[60]), "multiple of 8"),
+        (dict(N=256, Ms=[0], Ks=[64]), "positive"),
+        (dict(N=256, Ms=[64], Ks=[64], B=0x20008), "16-byte aligned"),
+        (dict(N=256, Ms=[64], Ks=[64], A=0x30004), "16-byte aligned"),
+    ]
+    for kw, text in cases:
+        assert call(**kw) == fg.FG_ERR_INVALID, kw
+        assert text in fg.last_error(), (kw, fg.last_error())
+
+
 def test_settings_round_trip(fg):
     fg.set_semantics("math")
     assert fg.get_semantics() == fg.FG_SEM_MATH
