@@ -123,6 +123,35 @@ def test_noalloc_arguments_checked_before_device_work(fg):
         assert text in fg.last_error(), (kw, fg.last_error())
 
 
+def test_device_chain_arguments_checked_before_device_work(fg):
+    """fg_chain_dev refuses unknown dtypes, bad chains, odd K and unaligned operands on
+    the host, and returns at once for N == 0 (addresses never dereferenced)."""
+    import ctypes
+    L = fg.lib()
+
+    def call(dt, N, Ms, Ks, C=0x10000, B=0x20000, A=0x30000):
+        n = len(Ms)
+        As = (ctypes.c_void_p * max(n, 1))(*[A + 0x1000 * i for i in range(n)])
+        Mv = (ctypes.c_long * max(n, 1))(*Ms)
+        Kv = (ctypes.c_long * max(n, 1))(*Ks)
+        return L.fg_chain_dev(dt, C, B, N, n, ctypes.cast(As, ctypes.c_void_p),
+                              ctypes.cast(Mv, ctypes.c_void_p), ctypes.cast(Kv, ctypes.c_void_p),
+                              None)
+
+    cases = [
+        (dict(dt=7, N=256, Ms=[64], Ks=[64]), "dtype"),
+        (dict(dt=fg.FG_DT_BF16, N=256, Ms=[], Ks=[]), "num_gemm"),
+        (dict(dt=fg.FG_DT_INT8, N=256, Ms=[64, 32], Ks=[64, 48]), "previous M"),
+        (dict(dt=fg.FG_DT_BF16, N=256, Ms=[64], Ks=[63]), "multiple of 2"),
+        (dict(dt=fg.FG_DT_F32, N=(1 << 30) + 1, Ms=[64], Ks=[64]), "too large"),
+        (dict(dt=fg.FG_DT_BF16, N=256, Ms=[64], Ks=[64], C=0x10004), "16-byte aligned"),
+    ]
+    for kw, text in cases:
+        assert call(**kw) == fg.FG_ERR_INVALID, kw
+        assert text in fg.last_error(), (kw, fg.last_error())
+    assert call(fg.FG_DT_BF16, 0, [64], [64]) == fg.FG_OK
+
+
 def test_settings_round_trip(fg):
     fg.set_semantics("math")
     assert fg.get_semantics() == fg.FG_SEM_MATH
